@@ -1,0 +1,154 @@
+/*
+ * Phase-retrieval API: drop-in for the reference's include/spimage/phasing.h.
+ *
+ * Enums, parameter structs and the SpPhaser field prefix up to gp keep the
+ * reference's layout (phasing.h:14-91), because callers set ph->algorithm /
+ * ph->sup_algorithm and read ph->model directly.  The private tail is one
+ * opaque pointer to the device context.  Every iteration runs on the GPU
+ * (SpEngineCUDA); there is no CPU engine in this library: SpEngineCPU makes
+ * sp_phaser_init return -3 instead of silently running elsewhere.
+ */
+#ifndef SPB_PHASING_H
+#define SPB_PHASING_H 1
+#include "image.h"
+#include "map.h"
+#include "support_update.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SpModelRandomPhases = 1,
+  SpModelZeroPhases = 2,
+  SpModelRandomValues = 4,
+  SpModelMaskedOutZeroed = 256
+} SpModelInitialization;
+typedef enum { SpSupportFromPatterson = 1 } SpSupportInitialization;
+typedef enum { SpHIO = 1, SpRAAR, SpDiffMap, SpER } SpPhasingAlgorithmType;
+typedef enum {
+  SpNoConstraints = 0,
+  SpRealObject = 1,
+  SpPositiveRealObject = 2,
+  SpPositiveComplexObject = 4,
+  SpPositivityFlipping = 8,
+  SpCentrosymmetricObject = 16,
+  SpAmplitudeErrorMargin = 32
+} SpPhasingConstraints;
+typedef enum { SpEngineAutomatic = 0, SpEngineCPU = 1, SpEngineCUDA = 2 } SpPhasingEngine;
+typedef enum { SpPixelInsideSupport = 1, SpPixelMeasuredAmplitude = 2 } SpPhasingPixelFlags;
+typedef enum { SpRecoverPhases = 0, SpRecoverAmplitudes = 1 } SpPhasingObjective;
+
+typedef struct {
+  sp_smap *beta;
+  SpPhasingConstraints constraints;
+} SpPhasingHIOParameters;
+typedef struct {
+  SpPhasingConstraints constraints;
+} SpPhasingERParameters;
+typedef SpPhasingHIOParameters SpPhasingRAARParameters;
+typedef struct {
+  sp_smap *beta;
+  real gamma1;
+  real gamma2;
+  SpPhasingConstraints constraints;
+} SpPhasingDiffMapParameters;
+typedef struct {
+  SpPhasingAlgorithmType type;
+  void *params;
+} SpPhasingAlgorithm;
+
+typedef struct {
+  sp_3matrix *amplitudes;
+  sp_3matrix *amplitudes_min;
+  sp_3matrix *amplitudes_max;
+  sp_c3matrix *phased_amplitudes;
+  sp_i3matrix *pixel_flags;
+  SpPhasingObjective phasing_objective;
+  SpPhasingAlgorithm *algorithm;
+  SpSupportArray *sup_algorithm;
+  int iteration;
+  int image_size;
+  int nx;
+  int ny;
+  int nz;
+  Image *model;
+  int model_iteration;
+  Image *old_model;
+  int old_model_iteration;
+  Image *model_change;
+  int model_change_iteration;
+  Image *support;
+  int support_iteration;
+  Image *amplitudes_image;
+  Image *fmodel;
+  int fmodel_iteration;
+  Image *model_before_projection;
+  int model_before_projection_iteration;
+  SpPhasingEngine engine;
+  Image *g0; /* unused by the GPU engine (NULL), kept for layout */
+  Image *g1;
+  Image *gp;
+  void *device; /* opaque spb_ctx */
+} SpPhaser;
+
+/* phasing.c:16-76 */
+SpPhasingAlgorithm *sp_phasing_hio_alloc(sp_smap *beta, SpPhasingConstraints constraints);
+SpPhasingAlgorithm *sp_phasing_raar_alloc(sp_smap *beta, SpPhasingConstraints constraints);
+SpPhasingAlgorithm *sp_phasing_diff_map_alloc(sp_smap *beta, real gamma1, real gamma2,
+                                              SpPhasingConstraints constraints);
+SpPhasingAlgorithm *sp_phasing_er_alloc(SpPhasingConstraints constraints);
+
+/* phasing.c:78-186 */
+SpPhaser *sp_phaser_alloc(void);
+void sp_phaser_free(SpPhaser *ph);
+
+/* phasing.c:365-554: host copies cached per iteration */
+const Image *sp_phaser_model(SpPhaser *ph);
+const Image *sp_phaser_model_with_support(SpPhaser *ph);
+const Image *sp_phaser_model_before_projection(SpPhaser *ph);
+const Image *sp_phaser_old_model(SpPhaser *ph);
+const Image *sp_phaser_fmodel(SpPhaser *ph);
+const Image *sp_phaser_fmodel_with_mask(SpPhaser *ph);
+Image *sp_phaser_model_change(SpPhaser *ph);
+const Image *sp_phaser_support(SpPhaser *ph);
+const Image *sp_phaser_amplitudes(SpPhaser *ph);
+
+/* phasing.c:803-893 */
+real sp_phaser_ereal(SpPhaser *ph);
+real sp_phaser_efourier(SpPhaser *ph, real *FcFo);
+real sp_phaser_support_fraction(SpPhaser *ph);
+
+/* phasing.c:189-363 */
+void sp_phaser_set_model(SpPhaser *ph, const Image *model);
+void sp_phaser_set_support(SpPhaser *ph, const Image *support);
+void sp_phaser_set_phased_amplitudes(SpPhaser *ph, const Image *phased_amplitudes);
+void sp_phaser_set_amplitudes(SpPhaser *ph, const Image *amplitudes);
+void sp_phaser_set_amplitudes_margins(SpPhaser *ph, const Image *amplitudes_min, const Image *amplitudes_max);
+
+/* phasing.c:558-604 */
+int sp_phaser_init(SpPhaser *ph, SpPhasingAlgorithm *alg, SpSupportArray *sup_alg, SpPhasingEngine engine);
+int sp_phaser_set_phasing_algorithm(SpPhaser *ph, SpPhasingAlgorithm *alg);
+int sp_phaser_set_support_algorithm(SpPhaser *ph, SpSupportArray *alg);
+/* phasing.c:606-724 */
+int sp_phaser_init_model(SpPhaser *ph, const Image *model, int flags);
+/* phasing.c:727-778 */
+int sp_phaser_init_support(SpPhaser *ph, const Image *support, int flags, real value);
+/* phasing.c:895-1024 */
+int sp_phaser_iterate(SpPhaser *ph, int iterations);
+void sp_phaser_set_objective(SpPhaser *ph, SpPhasingObjective obj);
+
+/* support updates, support_update.c:124-179 (GPU) */
+int sp_support_area_update_support(SpSupportAlgorithm *alg, SpPhaser *ph);
+int sp_support_threshold_update_support(SpSupportAlgorithm *alg, SpPhaser *ph);
+int sp_support_static_update_support(SpSupportAlgorithm *alg, SpPhaser *ph);
+/* support_update.c:489-494 */
+int sp_support_array_update(SpSupportArray *array, SpPhaser *ph);
+
+/* Not in the reference: message of the last device error seen by this
+ * library (the reference calls exit()/abort() on device errors instead). */
+const char *sp_phaser_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,98 @@
+/*
+ * Thin C-ABI device layer under the phasing API (libspimage_b200.so).
+ *
+ * Plain pointers and sizes only.  The host C library (sp_phaser_* etc.) calls
+ * these; an FFI binding may call them directly too.  Complex arrays are
+ * interleaved float pairs (re, im), x fastest, zero frequency at index 0 --
+ * the layout of the reference's Image data.  Return value 0 is success, a
+ * negative value an error whose text spb_error_string() returns.  Calls that
+ * return data to host memory synchronise the context's stream; the others
+ * only enqueue work.
+ *
+ * Replaces the reference's CUDA engine entry points (src/phasing.cu,
+ * src/support_update_cuda.cu, src/image_filter_cuda.cu, src/fft.cu) which call
+ * cuFFT, Thrust and cuRAND; here every kernel is this library's own.
+ */
+#ifndef SPB_DEVICE_H
+#define SPB_DEVICE_H 1
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct spb_ctx spb_ctx;
+
+typedef struct {
+  int algorithm;   /* 1 HIO, 2 RAAR, 3 difference map, 4 ER (SpPhasingAlgorithmType) */
+  int constraints; /* SpPhasingConstraints bits */
+  int objective;   /* 0 recover phases, 1 recover amplitudes */
+  float gamma1;    /* difference map only */
+  float gamma2;
+} spb_alg_desc;
+
+enum { SPB_SUPPORT_THRESHOLD = 1, SPB_SUPPORT_AREA = 2 };
+enum { SPB_G0 = 0, SPB_G1 = 1, SPB_GP = 2, SPB_FMODEL = 3 };
+
+/* Message of the last error on this thread ("" if none). */
+const char *spb_error_string(void);
+/* Number of usable CUDA devices (0 when there is none or the driver fails). */
+int spb_device_count(void);
+
+/* Context for one nx*ny*nz problem on the current CUDA device; replaces the
+ * device buffers the reference allocates in sp_phaser_set_amplitudes and
+ * sp_phaser_init_model (src/phasing.c:322-330,706-721). */
+int spb_ctx_create(spb_ctx **ctx, int nx, int ny, int nz);
+void spb_ctx_destroy(spb_ctx *ctx);
+int spb_ctx_synchronize(spb_ctx *ctx);
+
+/* Host -> device copies of the phaser inputs (src/phasing.c:189-363). */
+int spb_ctx_set_amplitudes(spb_ctx *ctx, const float *amp);
+int spb_ctx_set_margins(spb_ctx *ctx, const float *amp_min, const float *amp_max);
+int spb_ctx_set_phased_amplitudes(spb_ctx *ctx, const float *phased_amp);
+/* pixel flags as the reference's int32 SpPhasingPixelFlags bits */
+int spb_ctx_set_flags(spb_ctx *ctx, const int *flags);
+int spb_ctx_get_flags(spb_ctx *ctx, int *flags);
+
+/* Model initialisation (src/phasing.c:606-724; CUDA src/phasing.cu:184-240):
+ * set_model copies g1; model_from_fourier sets g1 = IFFT(F)/N; both clear g0
+ * and gp when reset_others is 1.  mask_out_unmeasured replaces g1 by
+ * IFFT(FFT(g1) with unmeasured pixels zeroed)/N (SpModelMaskedOutZeroed). */
+int spb_ctx_set_model(spb_ctx *ctx, const float *model, int reset_others);
+int spb_ctx_model_from_fourier(spb_ctx *ctx, const float *fourier, int reset_others);
+int spb_ctx_mask_out_unmeasured(spb_ctx *ctx);
+
+/* `iterations` phasing iterations of one algorithm (src/phasing.c:1111-1274;
+ * CUDA src/phasing.cu:40-182); beta[i] is the schedule value of iteration i
+ * (ignored for ER).  keep_gp = 1 stores the last iteration's model before
+ * projection for sp_phaser_model_before_projection / sp_phaser_ereal. */
+int spb_ctx_iterate(spb_ctx *ctx, const spb_alg_desc *alg, const float *beta, int iterations, int keep_gp);
+
+/* Support update from the current model (src/support_update.c:136-179):
+ * blur |g1| with `radius`, then threshold at the area quantile (type AREA,
+ * value = area fraction) or at max*value (type THRESHOLD). */
+int spb_ctx_support_update(spb_ctx *ctx, int type, float radius, float value);
+/* SpSupportFromPatterson (src/phasing.c:744-763) */
+int spb_ctx_support_patterson(spb_ctx *ctx, float value);
+
+/* Device -> host copies: SPB_G0 (old model), SPB_G1 (model), SPB_GP (model
+ * before projection), SPB_FMODEL (FFT of the model, computed on the GPU). */
+int spb_ctx_get_image(spb_ctx *ctx, int which, float *out);
+/* Reductions in double: efourier sums {nom, den, FcFo num, FcFo den}
+ * (src/phasing.c:852-891); ereal sums {nom, den} (src/phasing.c:803-832). */
+int spb_ctx_efourier_sums(spb_ctx *ctx, double sums[4]);
+int spb_ctx_ereal_sums(spb_ctx *ctx, double sums[2]);
+int spb_ctx_support_count(spb_ctx *ctx, long long *count);
+
+/* One-shot transforms of host buffers (sp_image_fft/ifft, src/fft.c:53-189,
+ * src/fft.cu:7-43; sp_gaussian_blur, src/image_filter.c:80-90).  sign -1 is
+ * forward, +1 backward (unnormalised). */
+int spb_fft_host(int nx, int ny, int nz, int sign, const float *in, float *out);
+int spb_blur_host(int nx, int ny, int nz, const float *in, float radius, float *out);
+/* Support mask from an already blurred image (support_from_absolute_threshold,
+ * src/support_update.c:392-400 with the area rule :143-144 or the threshold
+ * rule :175-176): updates bit 0 of flags in place. */
+int spb_support_from_blur_host(long long n, const float *blur, int type, float value, int *flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,88 @@
+"""Builds libspimage_b200.so in-tree (sm_100a CUDA kernels + host C library).
+
+    python -m libspimage_b200.build [--force]
+
+CUDA sources are compiled by nvcc for sm_100a only; host C sources by gcc.
+Floating-point contraction is disabled everywhere on the phasing path
+(-fmad=false / -ffp-contract=off): the kernels spell out every rounding so the
+iterates reproduce the reference CPU engine's arithmetic.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libspimage_b200.so")
+
+CU_SOURCES = ["spb_kernels.cu", "spb_capi.cu"]
+C_SOURCES = ["host/image.c", "host/phasing.c", "host/support_update.c", "host/fft.c"]
+HEADERS = ["spb_fft.cuh", "spb_internal.h"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xptxas", "-O3"]
+CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wno-unused-function"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libspimage_b200")
+
+
+def _newer(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    return r
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    nvcc = _nvcc()
+    headers = [os.path.join(CSRC, h) for h in HEADERS] + [
+        os.path.join(INCLUDE, "spimage", f) for f in os.listdir(os.path.join(INCLUDE, "spimage"))
+    ]
+    objs = []
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, os.path.basename(src) + ".o")
+        objs.append(o)
+        if force or _newer(o, [s] + headers):
+            cmd = [nvcc] + ARCH + NVCC_FLAGS + ["-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+    for src in C_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, os.path.basename(src) + ".o")
+        objs.append(o)
+        if force or _newer(o, [s] + headers):
+            cmd = ["gcc"] + CC_FLAGS + ["-I", INCLUDE, "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+    if force or _newer(LIB, objs):
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lm"]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,158 @@
+/*
+ * Image and matrix lifecycle helpers of the phasing path (host C).
+ * Behaviour follows the reference: src/linear_alg.c:84-125 (calloc'd
+ * matrices), src/image_util.c:1223-1300 (alloc/duplicate/free),
+ * :2322-2326 (memcpy), :1035-1067 (dephase/rephase), :120-127 (sp_srand,
+ * p_drand48 over glibc rand()).
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "spimage.h"
+
+sp_3matrix *_sp_3matrix_alloc(unsigned int nx, unsigned int ny, unsigned int nz, const char *file, int line) {
+  (void)file; (void)line;
+  sp_3matrix *m = (sp_3matrix *)malloc(sizeof(sp_3matrix));
+  m->x = nx; m->y = ny; m->z = nz;
+  m->data = (real *)calloc((size_t)nx * ny * nz, sizeof(real));
+  return m;
+}
+
+sp_i3matrix *_sp_i3matrix_alloc(unsigned int nx, unsigned int ny, unsigned int nz, const char *file, int line) {
+  (void)file; (void)line;
+  sp_i3matrix *m = (sp_i3matrix *)malloc(sizeof(sp_i3matrix));
+  m->x = nx; m->y = ny; m->z = nz;
+  m->data = (int *)calloc((size_t)nx * ny * nz, sizeof(int));
+  return m;
+}
+
+sp_c3matrix *_sp_c3matrix_alloc(unsigned int nx, unsigned int ny, unsigned int nz, const char *file, int line) {
+  (void)file; (void)line;
+  sp_c3matrix *m = (sp_c3matrix *)malloc(sizeof(sp_c3matrix));
+  m->x = nx; m->y = ny; m->z = nz;
+  m->data = (Complex *)calloc((size_t)nx * ny * nz, sizeof(Complex));
+  return m;
+}
+
+void _sp_3matrix_free(sp_3matrix *m, const char *file, int line) {
+  (void)file; (void)line;
+  if (!m) return;
+  free(m->data);
+  free(m);
+}
+void _sp_i3matrix_free(sp_i3matrix *m, const char *file, int line) {
+  (void)file; (void)line;
+  if (!m) return;
+  free(m->data);
+  free(m);
+}
+void _sp_c3matrix_free(sp_c3matrix *m, const char *file, int line) {
+  (void)file; (void)line;
+  if (!m) return;
+  free(m->data);
+  free(m);
+}
+
+Image *_sp_image_alloc(int x, int y, int z, const char *file, int line) {
+  if (x < 1 || y < 1 || z < 1) {
+    fprintf(stderr, "Dimensions must be positive integers\n");
+    abort();
+  }
+  Image *r = (Image *)malloc(sizeof(Image));
+  r->detector = (Detector *)calloc(1, sizeof(Detector));
+  r->detector->image_center[0] = (x - 1) / 2.0;
+  r->detector->image_center[1] = (y - 1) / 2.0;
+  r->detector->image_center[2] = (z - 1) / 2.0;
+  r->detector->orientation = NULL;
+  r->mask = _sp_i3matrix_alloc(x, y, z, file, line);
+  r->image = _sp_c3matrix_alloc(x, y, z, file, line);
+  r->scaled = 0;
+  r->shifted = 0;
+  r->phased = 0;
+  r->rec_coords = NULL;
+  r->num_dimensions = z == 1 ? SP_2D : SP_3D;
+  return r;
+}
+
+Image *_sp_image_duplicate(const Image *in, int flags, const char *file, int line) {
+  Image *r = (Image *)malloc(sizeof(Image));
+  memcpy(r, in, sizeof(Image));
+  r->detector = (Detector *)malloc(sizeof(Detector));
+  memcpy(r->detector, in->detector, sizeof(Detector));
+  r->image = _sp_c3matrix_alloc(in->image->x, in->image->y, in->image->z, file, line);
+  if (flags & SP_COPY_DATA)
+    memcpy(r->image->data, in->image->data, sizeof(Complex) * (size_t)sp_image_size(in));
+  r->mask = _sp_i3matrix_alloc(in->image->x, in->image->y, in->image->z, file, line);
+  if (flags & SP_COPY_MASK) memcpy(r->mask->data, in->mask->data, sizeof(int) * (size_t)sp_image_size(in));
+  return r;
+}
+
+void _sp_image_free(Image *in, const char *file, int line) {
+  if (!in) return;
+  _sp_c3matrix_free(in->image, file, line);
+  _sp_i3matrix_free(in->mask, file, line);
+  free(in->detector);
+  free(in);
+}
+
+void sp_image_memcpy(Image *dst, const Image *src) {
+  memcpy(dst->mask->data, src->mask->data, sizeof(int) * (size_t)sp_image_size(src));
+  memcpy(dst->image->data, src->image->data, sizeof(Complex) * (size_t)sp_image_size(src));
+  memcpy(dst->detector, src->detector, sizeof(Detector));
+}
+
+void sp_image_fill(Image *a, Complex value) {
+  const long long n = sp_image_size(a);
+  for (long long i = 0; i < n; i++) a->image->data[i] = value;
+}
+
+/* complex multiply by (value, 0), as src/image_util.c:1967-1970 */
+void sp_image_scale(Image *img, real value) {
+  const long long n = sp_image_size(img);
+  for (long long i = 0; i < n; i++) {
+    const Complex a = img->image->data[i];
+    img->image->data[i].re = a.re * value - a.im * 0.0f;
+    img->image->data[i].im = a.re * 0.0f + value * a.im;
+  }
+}
+
+void sp_image_dephase(Image *img) {
+  img->phased = 0;
+  const long long n = sp_image_size(img);
+  for (long long i = 0; i < n; i++) {
+    img->image->data[i].re = sp_cabs(img->image->data[i]);
+    img->image->data[i].im = 0;
+  }
+}
+
+void sp_srand(int i) { srand((unsigned)i); }
+
+real p_drand48(void) { return (real)(((double)rand()) / (double)RAND_MAX); }
+
+void sp_image_rephase(Image *img, int type) {
+  img->phased = 1;
+  const long long n = sp_image_size(img);
+  if (type == SP_ZERO_PHASE) {
+    for (long long i = 0; i < n; i++) img->image->data[i] = sp_cinit(sp_cabs(img->image->data[i]), 0);
+  } else if (type == SP_RANDOM_PHASE) {
+    for (long long i = 0; i < n; i++) {
+      const real phase = p_drand48() * 3.14159265358979323846 * 2;
+      const real amp = sp_cabs(img->image->data[i]);
+      img->image->data[i].re = cos(phase) * amp;
+      img->image->data[i].im = sin(phase) * amp;
+    }
+  }
+}
+
+/* ---- FFI helpers: sp_smap's constructors are static inline in map.h, so a
+ * foreign-function binding (ctypes, cffi) has no symbol to call; these give
+ * it one. ---- */
+sp_smap *spb_smap_create(int n, const real *keys, const real *values) {
+  sp_smap *m = sp_smap_alloc(n > 0 ? (unsigned)n : 1u);
+  for (int i = 0; i < n; i++) sp_smap_insert(m, keys[i], values[i]);
+  return m;
+}
+void spb_smap_free(sp_smap *m) { sp_smap_free(m); }
+real spb_smap_interpolate(sp_smap *m, real x) { return sp_smap_interpolate(m, x); }

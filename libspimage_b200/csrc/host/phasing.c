@@ -1,0 +1,581 @@
+/*
+ * SpPhaser API (host C) over the device layer (include/spimage/spb_device.h).
+ *
+ * Mirrors the reference's src/phasing.c: same entry points, argument meaning,
+ * return codes and caching of host-side images per iteration.  The phasing
+ * engine is always the GPU one; host copies of the inputs (amplitudes, pixel
+ * flags, ...) are kept like the reference does and uploaded lazily before
+ * device work.  Device errors are reported by return code (-8) and by
+ * sp_phaser_last_error() instead of exit()/abort().
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "spimage.h"
+#include "spimage/spb_device.h"
+
+typedef struct {
+  spb_ctx *ctx;
+  int amp_dirty, flags_dirty, margins_dirty, pamp_dirty;
+  int flags_dev_newer; /* device flags changed by a support update */
+} dev_state;
+
+static char g_last_err[512];
+
+const char *sp_phaser_last_error(void) { return g_last_err; }
+
+static int dev_error(const char *where) {
+  snprintf(g_last_err, sizeof(g_last_err), "%s: %s", where, spb_error_string());
+  fprintf(stderr, "spimage-b200: %s\n", g_last_err);
+  return -8;
+}
+
+static dev_state *state(SpPhaser *ph) {
+  if (!ph->device) ph->device = calloc(1, sizeof(dev_state));
+  return (dev_state *)ph->device;
+}
+
+static int ensure_ctx(SpPhaser *ph) {
+  dev_state *s = state(ph);
+  if (s->ctx) return 0;
+  if (!ph->nx) {
+    snprintf(g_last_err, sizeof(g_last_err), "phaser dimensions are not set");
+    return -8;
+  }
+  if (spb_ctx_create(&s->ctx, ph->nx, ph->ny, ph->nz)) return dev_error("device context");
+  s->amp_dirty = ph->amplitudes != NULL;
+  s->flags_dirty = ph->pixel_flags != NULL;
+  s->margins_dirty = ph->amplitudes_min != NULL;
+  s->pamp_dirty = ph->phased_amplitudes != NULL;
+  return 0;
+}
+
+/* pull support bits changed on the device before the host edits the flags */
+static int sync_flags_to_host(SpPhaser *ph) {
+  dev_state *s = state(ph);
+  if (!s->ctx || !s->flags_dev_newer || !ph->pixel_flags) return 0;
+  if (spb_ctx_get_flags(s->ctx, ph->pixel_flags->data)) return dev_error("download pixel flags");
+  s->flags_dev_newer = 0;
+  return 0;
+}
+
+static int sync_to_device(SpPhaser *ph) {
+  if (ensure_ctx(ph)) return -8;
+  dev_state *s = state(ph);
+  if (s->amp_dirty && ph->amplitudes) {
+    if (spb_ctx_set_amplitudes(s->ctx, ph->amplitudes->data)) return dev_error("upload amplitudes");
+    s->amp_dirty = 0;
+  }
+  if (s->flags_dirty && ph->pixel_flags) {
+    if (spb_ctx_set_flags(s->ctx, ph->pixel_flags->data)) return dev_error("upload pixel flags");
+    s->flags_dirty = 0;
+  }
+  if (s->margins_dirty && ph->amplitudes_min && ph->amplitudes_max) {
+    if (spb_ctx_set_margins(s->ctx, ph->amplitudes_min->data, ph->amplitudes_max->data))
+      return dev_error("upload amplitude margins");
+    s->margins_dirty = 0;
+  }
+  if (s->pamp_dirty && ph->phased_amplitudes) {
+    if (spb_ctx_set_phased_amplitudes(s->ctx, (const float *)ph->phased_amplitudes->data))
+      return dev_error("upload phased amplitudes");
+    s->pamp_dirty = 0;
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------- algorithms */
+
+/* phasing.c:16-45: gamma1 = INFINITY selects Elser's optimal gammas at beta(0) */
+SpPhasingAlgorithm *sp_phasing_diff_map_alloc(sp_smap *beta, real gamma1, real gamma2,
+                                              SpPhasingConstraints constraints) {
+  SpPhasingAlgorithm *ret = (SpPhasingAlgorithm *)malloc(sizeof(SpPhasingAlgorithm));
+  SpPhasingDiffMapParameters *p = (SpPhasingDiffMapParameters *)malloc(sizeof(SpPhasingDiffMapParameters));
+  ret->type = SpDiffMap;
+  p->beta = beta;
+  if (isinf(gamma1)) {
+    const real b = sp_smap_interpolate(p->beta, 0);
+    const real sigma = 0.1;
+    p->gamma1 = -(4 + (2 + b) * sigma + b * sigma * sigma) / (b * (4 - sigma + sigma * sigma));
+    p->gamma2 = (3 - b) / (2 * b);
+  } else {
+    p->gamma1 = gamma1;
+    p->gamma2 = gamma2;
+  }
+  p->constraints = constraints;
+  ret->params = p;
+  return ret;
+}
+
+static SpPhasingAlgorithm *beta_alg(SpPhasingAlgorithmType type, sp_smap *beta, SpPhasingConstraints c) {
+  SpPhasingAlgorithm *ret = (SpPhasingAlgorithm *)malloc(sizeof(SpPhasingAlgorithm));
+  SpPhasingHIOParameters *p = (SpPhasingHIOParameters *)malloc(sizeof(SpPhasingHIOParameters));
+  ret->type = type;
+  p->beta = beta;
+  p->constraints = c;
+  ret->params = p;
+  return ret;
+}
+
+SpPhasingAlgorithm *sp_phasing_raar_alloc(sp_smap *beta, SpPhasingConstraints constraints) {
+  return beta_alg(SpRAAR, beta, constraints);
+}
+
+SpPhasingAlgorithm *sp_phasing_hio_alloc(sp_smap *beta, SpPhasingConstraints constraints) {
+  return beta_alg(SpHIO, beta, constraints);
+}
+
+SpPhasingAlgorithm *sp_phasing_er_alloc(SpPhasingConstraints constraints) {
+  SpPhasingAlgorithm *ret = (SpPhasingAlgorithm *)malloc(sizeof(SpPhasingAlgorithm));
+  SpPhasingERParameters *p = (SpPhasingERParameters *)malloc(sizeof(SpPhasingERParameters));
+  ret->type = SpER;
+  p->constraints = constraints;
+  ret->params = p;
+  return ret;
+}
+
+/* ---------------------------------------------------------- construction */
+
+SpPhaser *sp_phaser_alloc(void) {
+  SpPhaser *ph = (SpPhaser *)calloc(1, sizeof(SpPhaser));
+  ph->model_iteration = -1;
+  ph->fmodel_iteration = -1;
+  ph->model_before_projection_iteration = -1;
+  ph->model_change_iteration = -1;
+  ph->support_iteration = -1;
+  ph->old_model_iteration = -1;
+  ph->phasing_objective = SpRecoverPhases;
+  return ph;
+}
+
+void sp_phaser_set_objective(SpPhaser *ph, SpPhasingObjective obj) { ph->phasing_objective = obj; }
+
+void sp_phaser_free(SpPhaser *ph) {
+  if (!ph) return;
+  Image **imgs[] = {&ph->model, &ph->model_before_projection, &ph->model_change, &ph->amplitudes_image,
+                    &ph->old_model, &ph->support, &ph->fmodel};
+  for (size_t i = 0; i < sizeof(imgs) / sizeof(imgs[0]); i++)
+    if (*imgs[i]) { sp_image_free(*imgs[i]); *imgs[i] = NULL; }
+  if (ph->amplitudes) sp_3matrix_free(ph->amplitudes);
+  if (ph->amplitudes_min) sp_3matrix_free(ph->amplitudes_min);
+  if (ph->amplitudes_max) sp_3matrix_free(ph->amplitudes_max);
+  if (ph->pixel_flags) sp_i3matrix_free(ph->pixel_flags);
+  if (ph->phased_amplitudes) sp_c3matrix_free(ph->phased_amplitudes);
+  if (ph->device) {
+    dev_state *s = (dev_state *)ph->device;
+    if (s->ctx) spb_ctx_destroy(s->ctx);
+    free(s);
+  }
+  free(ph);
+}
+
+/* phasing.c:271-292: first image fixes the shape; a mismatch aborts */
+static void phaser_check_dimensions(SpPhaser *ph, const Image *a) {
+  if (!ph->nx) {
+    ph->nx = sp_image_x(a);
+    ph->ny = sp_image_y(a);
+    ph->nz = sp_image_z(a);
+    ph->image_size = ph->nx * ph->ny * ph->nz;
+  }
+  if (ph->nx != sp_image_x(a) || ph->ny != sp_image_y(a) || ph->nz != sp_image_z(a)) {
+    fprintf(stderr, "spimage-b200: image shape %dx%dx%d does not match the phaser's %dx%dx%d\n", sp_image_x(a),
+            sp_image_y(a), sp_image_z(a), ph->nx, ph->ny, ph->nz);
+    abort();
+  }
+}
+
+static void ensure_flags(SpPhaser *ph) {
+  if (!ph->pixel_flags) ph->pixel_flags = sp_i3matrix_alloc(ph->nx, ph->ny, ph->nz);
+}
+
+/* phasing.c:189-204 */
+void sp_phaser_set_model(SpPhaser *ph, const Image *model) {
+  phaser_check_dimensions(ph, model);
+  ph->model_iteration = -1;
+  if (ensure_ctx(ph)) return;
+  if (spb_ctx_set_model(state(ph)->ctx, (const float *)model->image->data, 0)) dev_error("set model");
+}
+
+/* phasing.c:207-232 */
+void sp_phaser_set_support(SpPhaser *ph, const Image *support) {
+  phaser_check_dimensions(ph, support);
+  ph->support_iteration = -1;
+  ensure_flags(ph);
+  sync_flags_to_host(ph);
+  for (int i = 0; i < ph->image_size; i++) {
+    if (sp_real(support->image->data[i])) ph->pixel_flags->data[i] |= SpPixelInsideSupport;
+    else ph->pixel_flags->data[i] &= ~SpPixelInsideSupport;
+  }
+  state(ph)->flags_dirty = 1;
+}
+
+/* phasing.c:235-269 */
+void sp_phaser_set_phased_amplitudes(SpPhaser *ph, const Image *pa) {
+  phaser_check_dimensions(ph, pa);
+  if (!ph->phased_amplitudes) ph->phased_amplitudes = sp_c3matrix_alloc(ph->nx, ph->ny, ph->nz);
+  ensure_flags(ph);
+  sync_flags_to_host(ph);
+  for (int i = 0; i < ph->image_size; i++) {
+    ph->phased_amplitudes->data[i] = pa->image->data[i];
+    if (pa->mask->data[i]) ph->pixel_flags->data[i] |= SpPixelMeasuredAmplitude;
+    else ph->pixel_flags->data[i] &= ~SpPixelMeasuredAmplitude;
+  }
+  state(ph)->pamp_dirty = 1;
+  state(ph)->flags_dirty = 1;
+}
+
+/* phasing.c:294-333 */
+void sp_phaser_set_amplitudes(SpPhaser *ph, const Image *amplitudes) {
+  phaser_check_dimensions(ph, amplitudes);
+  if (!ph->amplitudes) ph->amplitudes = sp_3matrix_alloc(ph->nx, ph->ny, ph->nz);
+  ensure_flags(ph);
+  sync_flags_to_host(ph);
+  int masked = 0;
+  for (int i = 0; i < ph->image_size; i++) {
+    ph->amplitudes->data[i] = sp_real(amplitudes->image->data[i]);
+    if (amplitudes->mask->data[i]) {
+      ph->pixel_flags->data[i] |= SpPixelMeasuredAmplitude;
+      masked++;
+    } else {
+      ph->pixel_flags->data[i] &= ~SpPixelMeasuredAmplitude;
+    }
+  }
+  if (masked == 0) fprintf(stderr, "Amplitudes mask is all zeros!\n");
+  state(ph)->amp_dirty = 1;
+  state(ph)->flags_dirty = 1;
+}
+
+/* phasing.c:335-363 */
+void sp_phaser_set_amplitudes_margins(SpPhaser *ph, const Image *amin, const Image *amax) {
+  phaser_check_dimensions(ph, amin);
+  phaser_check_dimensions(ph, amax);
+  if (!ph->amplitudes_min) ph->amplitudes_min = sp_3matrix_alloc(ph->nx, ph->ny, ph->nz);
+  if (!ph->amplitudes_max) ph->amplitudes_max = sp_3matrix_alloc(ph->nx, ph->ny, ph->nz);
+  for (int i = 0; i < ph->image_size; i++) {
+    ph->amplitudes_min->data[i] = sp_real(amin->image->data[i]);
+    ph->amplitudes_max->data[i] = sp_real(amax->image->data[i]);
+  }
+  state(ph)->margins_dirty = 1;
+}
+
+/* ------------------------------------------------------------- accessors */
+
+const Image *sp_phaser_amplitudes(SpPhaser *ph) {
+  if (!ph->amplitudes_image) {
+    ph->amplitudes_image = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+    sync_flags_to_host(ph);
+    for (int i = 0; i < ph->image_size; i++) {
+      ph->amplitudes_image->image->data[i] = sp_cinit(ph->amplitudes->data[i], 0);
+      ph->amplitudes_image->mask->data[i] = (ph->pixel_flags->data[i] & SpPixelMeasuredAmplitude) ? 1 : 0;
+    }
+  }
+  return ph->amplitudes_image;
+}
+
+static Image *fetch(SpPhaser *ph, Image **slot, int *slot_iteration, int which) {
+  if (*slot_iteration != ph->iteration || !*slot) {
+    if (!*slot) *slot = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+    if (ensure_ctx(ph)) return NULL;
+    if (spb_ctx_get_image(state(ph)->ctx, which, (float *)(*slot)->image->data)) {
+      dev_error("download image");
+      return NULL;
+    }
+    *slot_iteration = ph->iteration;
+  }
+  return *slot;
+}
+
+static Image *model_nc(SpPhaser *ph) { return fetch(ph, &ph->model, &ph->model_iteration, SPB_G1); }
+
+const Image *sp_phaser_model(SpPhaser *ph) { return model_nc(ph); }
+
+const Image *sp_phaser_model_before_projection(SpPhaser *ph) {
+  return fetch(ph, &ph->model_before_projection, &ph->model_before_projection_iteration, SPB_GP);
+}
+
+const Image *sp_phaser_old_model(SpPhaser *ph) {
+  return fetch(ph, &ph->old_model, &ph->old_model_iteration, SPB_G0);
+}
+
+static Image *fmodel_nc(SpPhaser *ph) {
+  Image *f = fetch(ph, &ph->fmodel, &ph->fmodel_iteration, SPB_FMODEL);
+  if (f) f->phased = 1;
+  return f;
+}
+
+const Image *sp_phaser_fmodel(SpPhaser *ph) { return fmodel_nc(ph); }
+
+const Image *sp_phaser_fmodel_with_mask(SpPhaser *ph) {
+  Image *f = fmodel_nc(ph);
+  const Image *amp = sp_phaser_amplitudes(ph);
+  if (f) memcpy(f->mask->data, amp->mask->data, sizeof(int) * (size_t)ph->image_size);
+  return f;
+}
+
+/* phasing.c:532-554: model - old model */
+Image *sp_phaser_model_change(SpPhaser *ph) {
+  Image *m = model_nc(ph);
+  if (!m) return NULL;
+  if (ph->model_change_iteration != ph->iteration) {
+    const Image *old = sp_phaser_old_model(ph);
+    if (!old) return NULL;
+    ph->model_change_iteration = ph->iteration;
+    for (int i = 0; i < ph->image_size; i++) {
+      ph->model_change->image->data[i].re = m->image->data[i].re - old->image->data[i].re;
+      ph->model_change->image->data[i].im = m->image->data[i].im - old->image->data[i].im;
+    }
+  }
+  return ph->model_change;
+}
+
+const Image *sp_phaser_support(SpPhaser *ph) {
+  if (!ph->support) ph->support = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  if (ph->iteration != ph->support_iteration) {
+    if (sync_flags_to_host(ph)) return NULL;
+    ph->support_iteration = ph->iteration;
+    sp_image_fill(ph->support, sp_cinit(0, 0));
+    for (int i = 0; i < ph->image_size; i++)
+      if (ph->pixel_flags->data[i] & SpPixelInsideSupport) ph->support->image->data[i].re = 1;
+  }
+  return ph->support;
+}
+
+const Image *sp_phaser_model_with_support(SpPhaser *ph) {
+  Image *m = model_nc(ph);
+  const Image *s = sp_phaser_support(ph);
+  if (!m || !s) return m;
+  for (int i = 0; i < ph->image_size; i++)
+    m->mask->data[i] = (s->image->data[i].re == 0.0 && s->image->data[i].im == 0.0) ? 0 : 1;
+  return m;
+}
+
+/* ------------------------------------------------------------- init/run */
+
+/* phasing.c:558-586; this library has only the GPU engine */
+int sp_phaser_init(SpPhaser *ph, SpPhasingAlgorithm *alg, SpSupportArray *sup_alg, SpPhasingEngine engine) {
+  if (!ph) {
+    fprintf(stderr, "Phaser is NULL!\n");
+    return -1;
+  }
+  if (!alg) {
+    fprintf(stderr, "Algorithm is NULL!\n");
+    return -2;
+  }
+  ph->algorithm = alg;
+  ph->sup_algorithm = sup_alg;
+  ph->iteration = 0;
+  if (engine == SpEngineCPU) {
+    snprintf(g_last_err, sizeof(g_last_err), "SpEngineCPU requested: this library runs phasing on the GPU only");
+    fprintf(stderr, "spimage-b200: %s\n", g_last_err);
+    return -3;
+  }
+  if (spb_device_count() < 1) {
+    snprintf(g_last_err, sizeof(g_last_err), "no CUDA device available for the GPU phasing engine");
+    fprintf(stderr, "spimage-b200: %s\n", g_last_err);
+    return -3;
+  }
+  ph->engine = SpEngineCUDA;
+  return 0;
+}
+
+int sp_phaser_set_phasing_algorithm(SpPhaser *ph, SpPhasingAlgorithm *alg) {
+  if (!alg) {
+    fprintf(stderr, "Algorithm is NULL!\n");
+    return -2;
+  }
+  ph->algorithm = alg;
+  return 0;
+}
+
+int sp_phaser_set_support_algorithm(SpPhaser *ph, SpSupportArray *alg) {
+  if (!alg) {
+    fprintf(stderr, "Phasing algorithm is NULL!\n");
+    return -2;
+  }
+  ph->sup_algorithm = alg;
+  return 0;
+}
+
+/* phasing.c:606-724 with the CPU engine's semantics: the starting model is
+ * derived from the host RNG (glibc rand(), as p_drand48) exactly like the
+ * reference CPU engine, then transformed on the GPU. */
+int sp_phaser_init_model(SpPhaser *ph, const Image *user_model, int flags) {
+  if (!ph) return -1;
+  if (ph->engine != SpEngineCUDA) {
+    snprintf(g_last_err, sizeof(g_last_err), "sp_phaser_init must succeed before sp_phaser_init_model");
+    return -3;
+  }
+  if (ph->model) { sp_image_free(ph->model); ph->model = NULL; }
+  if (ph->model_change) { sp_image_free(ph->model_change); ph->model_change = NULL; }
+  if (!user_model && !(flags & (SpModelRandomPhases | SpModelZeroPhases | SpModelRandomValues))) return -3;
+  if (user_model) phaser_check_dimensions(ph, user_model);
+  if (sync_to_device(ph)) return -8;
+  spb_ctx *ctx = state(ph)->ctx;
+  const int n = ph->image_size;
+  int rc = 0;
+  if (user_model) {
+    rc = spb_ctx_set_model(ctx, (const float *)user_model->image->data, 1);
+  } else if (flags & (SpModelRandomPhases | SpModelZeroPhases)) {
+    Image *tmp = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+    for (int i = 0; i < n; i++) tmp->image->data[i].re = ph->amplitudes->data[i];
+    sp_image_rephase(tmp, (flags & SpModelRandomPhases) ? SP_RANDOM_PHASE : SP_ZERO_PHASE);
+    rc = spb_ctx_model_from_fourier(ctx, (const float *)tmp->image->data, 1);
+    sp_image_free(tmp);
+  } else {
+    /* SpModelRandomValues: uniform (re, im) in [-0.5, 0.5) scaled so that the
+     * squared norm matches the amplitudes' (phasing.c:674-690) */
+    Image *m = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+    double sum = 0;
+    for (int i = 0; i < n; i++) sum += ph->amplitudes->data[i] * ph->amplitudes->data[i];
+    sum /= n;
+    for (int i = 0; i < n; i++) {
+      /* the reference's sp_cinit(p_drand48()-0.5, p_drand48()-0.5) draws the
+       * imaginary part first under gcc's argument evaluation order */
+      const real im = p_drand48() - 0.5;
+      const real re = p_drand48() - 0.5;
+      m->image->data[i] = sp_cinit(re, im);
+    }
+    double msum = 0;
+    for (int i = 0; i < n; i++) msum += sp_cabs2(m->image->data[i]);
+    const real model_sum = (real)msum;
+    sp_image_scale(m, sqrt(sum / model_sum));
+    rc = spb_ctx_set_model(ctx, (const float *)m->image->data, 1);
+    sp_image_free(m);
+  }
+  if (!rc && (flags & SpModelMaskedOutZeroed)) rc = spb_ctx_mask_out_unmeasured(ctx);
+  if (rc) return dev_error("init model");
+  ph->model = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  if (spb_ctx_get_image(ctx, SPB_G1, (float *)ph->model->image->data)) return dev_error("download model");
+  ph->model->phased = 1;
+  ph->model_iteration = -1;
+  ph->model_change = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  return 0;
+}
+
+/* phasing.c:727-778 */
+int sp_phaser_init_support(SpPhaser *ph, const Image *support, int flags, real value) {
+  if (support) {
+    phaser_check_dimensions(ph, support);
+    ensure_flags(ph);
+    sync_flags_to_host(ph);
+    for (int i = 0; i < ph->image_size; i++) {
+      if (sp_real(support->image->data[i])) ph->pixel_flags->data[i] |= SpPixelInsideSupport;
+      else ph->pixel_flags->data[i] &= ~SpPixelInsideSupport;
+    }
+    state(ph)->flags_dirty = 1;
+    ph->support_iteration = -1;
+    return 0;
+  }
+  if (flags & SpSupportFromPatterson) {
+    ensure_flags(ph);
+    if (sync_to_device(ph)) return -8;
+    if (spb_ctx_support_patterson(state(ph)->ctx, value)) return dev_error("Patterson support");
+    state(ph)->flags_dev_newer = 1;
+    ph->support_iteration = -1;
+    return 0;
+  }
+  return -1;
+}
+
+/* `k` phasing iterations of the current algorithm on the device */
+static int run_phasing(SpPhaser *ph, int k) {
+  if (k <= 0) return 0;
+  const SpPhasingAlgorithm *alg = ph->algorithm;
+  spb_alg_desc d;
+  memset(&d, 0, sizeof(d));
+  d.algorithm = alg->type;
+  d.objective = ph->phasing_objective;
+  sp_smap *beta = NULL;
+  if (alg->type == SpHIO || alg->type == SpRAAR) {
+    const SpPhasingHIOParameters *p = (const SpPhasingHIOParameters *)alg->params;
+    beta = p->beta;
+    d.constraints = p->constraints;
+  } else if (alg->type == SpDiffMap) {
+    const SpPhasingDiffMapParameters *p = (const SpPhasingDiffMapParameters *)alg->params;
+    beta = p->beta;
+    d.constraints = p->constraints;
+    d.gamma1 = p->gamma1;
+    d.gamma2 = p->gamma2;
+    d.objective = SpRecoverPhases; /* the reference's difference map always projects on amplitudes */
+  } else {
+    d.constraints = ((const SpPhasingERParameters *)alg->params)->constraints;
+  }
+  float *b = (float *)malloc(sizeof(float) * (size_t)k);
+  for (int i = 0; i < k; i++) b[i] = beta ? sp_smap_interpolate(beta, ph->iteration + i) : 0.0f;
+  const int rc = spb_ctx_iterate(state(ph)->ctx, &d, b, k, 1);
+  free(b);
+  if (rc) return dev_error("iterate");
+  ph->iteration += k;
+  return 0;
+}
+
+/* phasing.c:895-1024 */
+int sp_phaser_iterate(SpPhaser *ph, int iterations) {
+  if (!ph) return -1;
+  if (!ph->algorithm) return -2;
+  if (!ph->model) return -3;
+  if ((!ph->amplitudes && ph->phasing_objective == SpRecoverPhases) ||
+      (!ph->phased_amplitudes && ph->phasing_objective == SpRecoverAmplitudes))
+    return -4;
+  if (!ph->pixel_flags) return -5;
+  if (!ph->model_change) return -6;
+  const int t = ph->algorithm->type;
+  if (t != SpHIO && t != SpRAAR && t != SpDiffMap && t != SpER) return -7;
+  if (ph->engine != SpEngineCUDA) return -8;
+  if (sync_to_device(ph)) return -8;
+  if (ph->sup_algorithm && ph->sup_algorithm->algorithms[0]->function) {
+    while (iterations) {
+      const int period = ph->sup_algorithm->update_period;
+      int to_update = period - 1 - ph->iteration % period;
+      const int to_iterate = (int)sp_min(iterations, to_update);
+      if (run_phasing(ph, to_iterate)) return -8;
+      iterations -= to_iterate;
+      to_update -= to_iterate;
+      if (to_update == 0 && iterations > 0) {
+        if (sp_support_array_update(ph->sup_algorithm, ph) < 0) return -8;
+        ph->iteration++;
+        iterations -= 1;
+      }
+    }
+  } else if (iterations) {
+    if (run_phasing(ph, iterations)) return -8;
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------- metrics */
+
+/* phasing.c:803-832 (sums in double on the device) */
+real sp_phaser_ereal(SpPhaser *ph) {
+  if (ensure_ctx(ph)) return -8;
+  double s[2];
+  if (spb_ctx_ereal_sums(state(ph)->ctx, s)) return dev_error("ereal");
+  return (real)sqrt(s[0] / s[1]);
+}
+
+/* phasing.c:852-891 */
+real sp_phaser_efourier(SpPhaser *ph, real *FcFo) {
+  if (sync_to_device(ph)) return -8;
+  double s[4];
+  if (spb_ctx_efourier_sums(state(ph)->ctx, s)) return dev_error("efourier");
+  if (FcFo) *FcFo = (real)(s[2] / s[3]);
+  return (real)sqrt(s[0] / s[1]);
+}
+
+/* phasing.c:834-850 */
+real sp_phaser_support_fraction(SpPhaser *ph) {
+  if (sync_to_device(ph)) return -8;
+  long long c = 0;
+  if (spb_ctx_support_count(state(ph)->ctx, &c)) return dev_error("support fraction");
+  return (real)c / (real)ph->image_size;
+}
+
+/* -------------------------------------------- hooks for support_update.c */
+
+int spb_phaser_support_update(SpPhaser *ph, int type, real radius, real value) {
+  if (sync_to_device(ph)) return -8;
+  if (spb_ctx_support_update(state(ph)->ctx, type, radius, value)) return dev_error("support update");
+  state(ph)->flags_dev_newer = 1;
+  return 0;
+}

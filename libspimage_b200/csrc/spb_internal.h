@@ -1,0 +1,100 @@
+// Internal device-layer declarations shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "spb_fft.cuh"
+
+namespace spb {
+
+// pixel flag bits kept per pixel on the device (uint8), same meaning as the
+// reference's SpPhasingPixelFlags (include/spimage/phasing.h:19)
+enum : uint8_t { FLAG_INSIDE = 1, FLAG_MEASURED = 2 };
+
+enum Alg : int { ALG_HIO = 1, ALG_RAAR = 2, ALG_DM = 3, ALG_ER = 4 };
+
+enum Constraint : int {
+  C_REAL = 1, C_POS_REAL = 2, C_POS_COMPLEX = 4, C_FLIP = 8, C_CENTROSYM = 16, C_MARGIN = 32
+};
+
+// Row-pass modes (lines along x, contiguous)
+enum RowMode : int {
+  ROW_FWD = 0,          // X = fwd_x(src)
+  ROW_FWD_DEPHASE = 1,  // X = fwd_x(|src| + 0i)
+  ROW_INV = 2,          // out = inv_x(src)
+  ROW_INV_SCALE = 3,    // out = inv_x(src) * (1/N) (complex multiply by (1/N, 0))
+  ROW_INV_ABS = 4,      // absout = |inv_x(src)|
+  ROW_ITER = 5,         // gp = inv_x(Y)/N; g1 = update(gp, g0); X = fwd_x(g1)
+  ROW_DM_F1_FWD = 6,    // Xf = fwd_x(f1(g)) with f1 = inside ? g : -gamma1*g
+  ROW_DM_ITER = 7,      // rho = inv_x(Y), f = inv_x(Yf); g1 = DM update; X = fwd_x(g1); Xf = fwd_x(f1(g1))
+  ROW_FWD_F32 = 8,      // X = fwd_x(real32 + 0i)
+  ROW_FWD_SQUARE_F32 = 9,  // X = fwd_x(real32^2 + 0i)
+};
+
+// Column-pass modes (lines along y or z, strided)
+enum ColMode : int {
+  COL_FWD = 0,
+  COL_INV = 1,
+  COL_PROJECT = 2,       // fwd, Fourier constraints + projection, inv
+  COL_PROJECT_NOFC = 3,  // fwd, projection only (difference-map f1), inv
+  COL_BLUR = 4,          // fwd, Gaussian multiplier, inv
+  COL_INV_SQUARE_F32 = 5,  // inv of (real32^2 + 0i) input (Patterson)
+};
+
+struct PassArgs {
+  // geometry
+  int nx, ny, nz;
+  long long n;  // nx*ny*nz
+  // line addressing for column passes: addr = o*ostride + c + i*estride
+  long long ostride, estride;
+  int ncols, nouter;
+  // buffers
+  const float2 *src;
+  const float2 *src2;  // second input line (DM: Yf)
+  const float2 *g0;    // previous iterate
+  float2 *dst;         // main output (X or out)
+  float2 *dst2;        // second output (DM: Xf)
+  float2 *g1;          // new iterate
+  float2 *gp;          // model before projection (optional)
+  float *absout;
+  const float *f32src;
+  const float *amp, *amp_min, *amp_max;
+  const float2 *phased_amp;
+  const uint8_t *flags;
+  // scalars
+  int alg, constraints, objective;
+  float beta, one_m2b, inv_n;
+  float gamma1, gamma2, one_p_g2, size_f;
+  // blur
+  double blur_c0;   // -2*pow(pi,2) (host glibc)
+  double blur_r2;   // pow(radius,2)
+  float nx_f;       // (float)nx
+  float n_f;        // (float)N
+};
+
+struct SelectState {
+  unsigned int prefix;       // key bits fixed so far
+  unsigned int prefix_mask;  // which bits are fixed
+  unsigned long long rank;   // remaining rank (0-based) within the prefix bucket, descending
+  unsigned int hist[2048];
+  float result;
+  unsigned int maxbits;
+};
+
+// host-side launchers (spb_kernels.cu)
+cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_mask_from_abs(const float *absv, const float *thr_dev, float rel, int use_rel, uint8_t *flags,
+                                 long long n, cudaStream_t st);
+cudaError_t launch_select_kth_desc(const float *absv, long long n, long long k, SelectState *state, cudaStream_t st);
+cudaError_t launch_max_abs(const float *absv, long long n, SelectState *state, cudaStream_t st);
+cudaError_t launch_reduce_efourier(const float2 *F, const float *amp, const uint8_t *flags, long long n,
+                                   double *out4, cudaStream_t st);
+cudaError_t launch_reduce_ereal(const float2 *gp, const uint8_t *flags, long long n, double *out2,
+                                cudaStream_t st);
+cudaError_t launch_count_inside(const uint8_t *flags, long long n, unsigned long long *out, cudaStream_t st);
+cudaError_t launch_flags_from_int(const int *src, uint8_t *dst, long long n, cudaStream_t st);
+cudaError_t launch_flags_to_int(const uint8_t *src, int *dst, long long n, cudaStream_t st);
+cudaError_t launch_scale_cmul(float2 *a, long long n, float v, cudaStream_t st);
+
+}  // namespace spb

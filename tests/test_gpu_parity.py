@@ -1,0 +1,94 @@
+"""GPU parity: every kernel path against the oracle (CPU restatement of the
+reference engine), through the library's C-ABI.  The device FFT and every
+pointwise step follow the same arithmetic as the oracle, so the checks are
+bit-exact unless a tolerance is written next to them."""
+import numpy as np
+import pytest
+
+from tests._engines import AREA, DIFFMAP, ER, HIO, RAAR, STATIC, THRESHOLD, bits, rel_l2, same_bits, setup
+
+pytestmark = pytest.mark.gpu
+
+FFT_SHAPES = [(8, 8), (16, 16), (32, 32), (64, 48), (24, 40), (17, 19), (128, 128), (256, 256), (192, 384),
+              (8, 16, 12), (16, 16, 16), (5, 7, 9), (1, 64), (1000, 8), (3, 1024)]
+
+
+@pytest.mark.parametrize("shape", FFT_SHAPES)
+@pytest.mark.parametrize("sign", [-1, 1])
+def test_fft_bit_exact(lib, oracle_mod, shape, sign):
+    rng = np.random.default_rng(hash(shape) % 1000)
+    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    got = lib.fft(x, sign)
+    want = oracle_mod.fft(x, sign)
+    assert same_bits(got, want), f"max abs diff {np.abs(got - want).max()}"
+
+
+@pytest.mark.parametrize("shape", [(32, 32), (64, 48), (8, 16, 12), (128, 128)])
+@pytest.mark.parametrize("radius", [0.7, 3.0])
+def test_blur_bit_exact(lib, oracle_mod, shape, radius):
+    rng = np.random.default_rng(7)
+    x = rng.random(shape).astype(np.complex64)
+    got = lib.gaussian_blur(x, radius)
+    want = oracle_mod.gaussian_blur(x, radius)
+    assert same_bits(got, want), f"rel {rel_l2(got, want)}"
+
+
+@pytest.mark.parametrize("area", [0.05, 0.1, 0.3333])
+def test_area_mask_bit_exact_on_identical_blur(lib, oracle_mod, area):
+    rng = np.random.default_rng(11)
+    blur = (rng.random((64, 64)) + 1j * rng.random((64, 64)) * 1e-3).astype(np.complex64)
+    blur.real[:4, :4] = 0.5  # ties at the threshold
+    flags = rng.integers(0, 4, size=blur.shape).astype(np.int32)
+    t = oracle_mod.area_threshold(blur, area)
+    # |.| exactly as the reference: sqrt(im*im + re*re) in float
+    a = np.sqrt((blur.imag * blur.imag + blur.real * blur.real).astype(np.float32))
+    want = (flags & ~1) | (a > np.float32(t)).astype(np.int32)
+    got = lib.support_from_blur(blur, AREA, area, flags)
+    assert np.array_equal(got, want)
+
+
+def test_threshold_mask_bit_exact_on_identical_blur(lib):
+    rng = np.random.default_rng(12)
+    blur = rng.random((48, 40)).astype(np.complex64)
+    flags = np.zeros(blur.shape, np.int32)
+    a = np.abs(blur.real).astype(np.float32)
+    want = (a > np.float32(a.max() * np.float32(0.2))).astype(np.int32)
+    got = lib.support_from_blur(blur, THRESHOLD, 0.2, flags)
+    assert np.array_equal(got, want)
+
+
+SCENARIOS = [
+    ("hio", (32, 32), HIO, None, 2),
+    ("raar", (32, 32), RAAR, None, 2),
+    ("er", (32, 32), ER, None, 2),
+    ("dm", (32, 32), DIFFMAP, None, 2),
+    ("hio_area", (64, 48), HIO, [(AREA, 5, {0: 3.0, 40: 0.7}, 0.1)], 2),
+    ("raar_thr", (24, 40), RAAR, [(THRESHOLD, 7, 2.0, 0.2)], 0),
+    ("er_area_3d", (8, 16, 12), ER, [(AREA, 5, 1.5, 0.2)], 2),
+    ("dm_area", (32, 32), DIFFMAP, [(AREA, 6, 2.0, 0.15)], 2),
+    ("hio_3d", (16, 16, 16), HIO, [(AREA, 10, 2.0, 0.1)], 2),
+    ("hio_nc", (48, 48), HIO, [(AREA, 9, 3.0, 0.1), (STATIC, 9, 0, 0)], 0),
+    ("raar_flip", (40, 30), RAAR, None, 2 | 8),
+    ("hio_complex", (32, 32), HIO, None, 4),
+    ("hio_real_centro", (32, 32), HIO, None, 1 | 16),
+]
+
+
+@pytest.mark.parametrize("name,shape,alg,sup,cons", SCENARIOS, ids=[s[0] for s in SCENARIOS])
+def test_phaser_bit_exact(lib, oracle_mod, name, shape, alg, sup, cons):
+    nit = 23
+    ref = setup(oracle_mod.Restatement(shape), shape, alg, sup, constraints=cons)
+    gpu = setup(lib.Phaser(shape), shape, alg, sup, constraints=cons)
+    assert same_bits(gpu.model(), ref.model()), "initial model"
+    assert ref.iterate(nit) == 0
+    assert gpu.iterate(nit) == 0
+    assert gpu.iteration == ref.iteration == nit
+    assert np.array_equal(gpu.support(), ref.support())
+    for which in (0, 1, 2):
+        g, r = gpu.get(which), ref.get(which)
+        assert same_bits(g, r), f"which={which} rel={rel_l2(g, r)}"
+    ef_g, fc_g = gpu.efourier()
+    ef_r, fc_r = ref.efourier()
+    assert abs(ef_g - ef_r) <= 1e-5 * abs(ef_r) + 1e-12
+    assert abs(gpu.ereal() - ref.ereal()) <= 1e-5 * abs(ref.ereal()) + 1e-12
+    assert gpu.support_fraction() == ref.support_fraction()
