@@ -1,0 +1,437 @@
+#!/usr/bin/env python
+"""Benchmark of the phase-retrieval hot path; prints ONE JSON line.
+
+Workload (default ``raar1024``): single-instance RAAR on a 1024x1024 FP32
+pattern (256x256 blob smoothed by sigma 2, 1e8 photons, Poisson, beamstop
+radius 8 px), 5000 RAAR iterations (beta 0.87, positive real object) with an
+area support update every 50 iterations (area 0.05, blur radius 3.0 -> 0.7),
+then 200 ER iterations.  One step = that whole reconstruction = 5200
+``sp_phaser_iterate`` iteration slots (a support update uses a slot, as in the
+reference).  Data are synthetic (seeded, ``libspimage_b200.synth``).
+
+value  : iteration slots / s with the inputs resident in HBM, device-timed with
+         CUDA events on the stream the kernels run on; L2 is flushed (256 MiB
+         write) before every timed step, outside the events.
+e2e    : the same metric through the C API with host buffers: set amplitudes,
+         random-phase start (host RNG as the reference), support, iterate,
+         read the model and the Fourier error back -- wall clock per step.
+Multi-GPU (torchrun): independent replicas, one per GPU (the path has no
+exchange step); value sums all ranks' slots over the slowest rank's time.
+
+``--impl reference`` times the reference's own CPU engine (oracle/_ref, built
+from the reference sources; the oracle restatement if that build is absent) on
+the host cores, each step a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "HIO/RAAR iters/sec, batched & served vs plain, at equal Fourier error; p50/p99"
+UNIT = "iterations/s"
+
+WORKLOADS = {
+    "raar1024": dict(
+        pattern="raar1024", shape=(1024, 1024), stages=[("RAAR", 0.87, 5000), ("ER", None, 200)], period=50,
+        area=0.05, blur={0: 3.0, 5000: 0.7}, constraints=2,
+        desc="single-instance RAAR 1024x1024 FP32: 5000 RAAR (beta 0.87, area support every 50, area 0.05, "
+             "blur 3.0->0.7) + 200 ER",
+    ),
+    "hio256": dict(
+        pattern="hio256", shape=(256, 256), stages=[("HIO", 0.9, 1000)], period=20, area=0.05,
+        blur={0: 3.0, 1000: 0.7}, constraints=2,
+        desc="plain HIO 256x256 FP32: 1000 HIO (beta 0.9, area support every 20, area 0.05, blur 3.0->0.7)",
+    ),
+}
+
+# algorithmic HBM bytes per pixel of the dominant 2-D kernels (bit-packed
+# support/measured masks): row pass reads Y + g_prev, writes g_new + X
+# (+ support bit); column pass reads X + amplitudes, writes Y (+ measured bit)
+ALGO_BYTES_PER_PIXEL = {"row_iter": 32.0 + 1.0 / 8, "col_project": 20.0 + 1.0 / 8}
+
+
+def slots_per_step(wl):
+    return sum(n for _, _, n in wl["stages"])
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms",
+                 "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 8:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, parts[4:8]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ------------------------------------------------------------------ GPU arm
+def build_phaser(L, wl, amp, mask, support, seed):
+    ph = L.Phaser(wl["shape"])
+    handles = []
+    for name, beta, _ in wl["stages"]:
+        alg = {"HIO": L.SpHIO, "RAAR": L.SpRAAR, "ER": L.SpER, "DM": L.SpDiffMap}[name]
+        ph.set_algorithm(alg, beta=beta if beta is not None else 0.9, constraints=wl["constraints"])
+        handles.append(ph.alg)
+    ph.alg = handles[0]
+    ph.add_support_update(L.SpSupportArea, wl["period"], wl["blur"], wl["area"])
+    ph.start()
+    ph.lib.sp_phaser_set_phasing_algorithm(ph.ph, handles[0])
+    ph.set_amplitudes(amp, mask)
+    rc = ph.init_model(L.SpModelRandomPhases, seed=seed)
+    assert rc == 0, rc
+    ph.set_support(support)
+    return ph, handles
+
+
+def run_stages(ph, handles, wl):
+    for h, (_, _, nit) in zip(handles, wl["stages"]):
+        ph.lib.sp_phaser_set_phasing_algorithm(ph.ph, h)
+        rc = ph.iterate(nit)
+        if rc:
+            raise RuntimeError(f"sp_phaser_iterate returned {rc}: {ph.lib.sp_phaser_last_error().decode()}")
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import libspimage_b200 as L
+    from libspimage_b200 import synth
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    wl = WORKLOADS[args.workload]
+    n = int(np.prod(wl["shape"]))
+    amp, mask, support, _ = synth.workload(wl["pattern"], seed=0)
+    L.load()
+    ph, handles = build_phaser(L, wl, amp, mask, support, seed=rank)
+    stream = torch.cuda.Stream()
+    ph.set_stream(stream.cuda_stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        run_stages(ph, handles, wl)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    evs = []
+    launches0 = ph.launch_count()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run_stages(ph, handles, wl)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    launches_total = ph.launch_count() - launches0
+    clocks = sampler.stop()
+    # one more step with a CUDA event pair around every kernel launch (direct
+    # launches, no graphs) for the per-kernel durations of the roofline
+    with torch.cuda.stream(stream):
+        flush.fill_(-1.0)
+    ph.profile(True)
+    run_stages(ph, handles, wl)
+    torch.cuda.synchronize()
+    ktimes = ph.kernel_times()
+    ph.profile(False)
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    slots = slots_per_step(wl)
+    value = world * args.steps * slots / (total_ms / 1e3)
+
+    # ---- end to end through the C API with host buffers
+    ph.set_stream(None)
+    del ph
+    e2e_val, h2d, d2h, efour = e2e_run(args, L, wl, amp, mask, support, rank, world, torch, dist)
+
+    # ---- roofline of the dominant kernel
+    peak, peak_kind = measured_peak()
+    dom = max(ktimes.items(), key=lambda kv: kv[1][1]) if ktimes else ("none", (0, 0.0))
+    name, (launches, ms) = dom
+    per_pixel = ALGO_BYTES_PER_PIXEL.get(name)
+    roof = None
+    if per_pixel and launches:
+        avg_s = ms / launches / 1e3
+        achieved = per_pixel * n / avg_s / 1e9
+        traffic = profiled_traffic(name, args.workload)
+        roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": traffic, "algorithmic_bytes_per_launch": per_pixel * n,
+                "avg_launch_us": round(avg_s * 1e6, 3)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(wl, args.cpu_sample_slots)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl["desc"], "shape": list(wl["shape"]), "slots_per_step": slots,
+                       "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before each timed step",
+                       "efourier_final_e2e": efour},
+            "e2e": {"value": round(e2e_val, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches_total),
+            "kernels": {k: {"launches": v[0], "avg_us": round(v[1] / max(v[0], 1) * 1e3, 3)} for k, v in ktimes.items()},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def e2e_run(args, L, wl, amp, mask, support, rank, world, torch, dist):
+    """Full user flow per step with host inputs; wall clock, max over ranks."""
+    import ctypes as C
+
+    n = int(np.prod(wl["shape"]))
+    ph = L.Phaser(wl["shape"])
+    handles = []
+    for name, beta, _ in wl["stages"]:
+        alg = {"HIO": L.SpHIO, "RAAR": L.SpRAAR, "ER": L.SpER, "DM": L.SpDiffMap}[name]
+        ph.set_algorithm(alg, beta=beta if beta is not None else 0.9, constraints=wl["constraints"])
+        handles.append(ph.alg)
+    ph.add_support_update(L.SpSupportArea, wl["period"], wl["blur"], wl["area"])
+    ph.start()
+    amp_img = L.new_image(np.asarray(amp, np.complex64), mask)
+    sup_img = L.new_image(np.asarray(support, np.complex64))
+    # user's input buffers live in pinned host memory
+    cudart = torch.cuda.cudart()
+    pinned = []
+    for img in (amp_img, sup_img):
+        for ptr, nbytes in ((img.contents.image.contents.data, 8 * n), (img.contents.mask.contents.data, 4 * n)):
+            if cudart.cudaHostRegister(ptr, nbytes, 0) == 0:
+                pinned.append(ptr)
+    lib = ph.lib
+    fc = C.c_float()
+    times, efour = [], None
+
+    def one(seed):
+        lib.sp_phaser_set_amplitudes(ph.ph, amp_img)
+        lib.sp_srand(seed)
+        assert lib.sp_phaser_init_model(ph.ph, None, L.SpModelRandomPhases) == 0
+        assert lib.sp_phaser_init_support(ph.ph, sup_img, 0, 0.0) == 0
+        run_stages(ph, handles, wl)
+        m = lib.sp_phaser_model(ph.ph)
+        assert m
+        return float(lib.sp_phaser_efourier(ph.ph, C.byref(fc)))
+
+    for w in range(args.warmup):
+        one(1000 + w)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        efour = one(rank * 1000 + k)
+        times.append(time.perf_counter() - t0)
+    total = float(sum(times))
+    if world > 1:
+        t = torch.tensor([total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    for ptr in pinned:
+        cudart.cudaHostUnregister(ptr)
+    ph.close()
+    L.free_image(amp_img)
+    L.free_image(sup_img)
+    slots = slots_per_step(wl)
+    # per step: amplitudes (4N) + pixel flags (1N) + random-phase start (8N) up; model (8N) down
+    h2d = 4 * n + n + 8 * n
+    d2h = 8 * n + 4 * 8
+    return world * args.steps * slots / total, h2d, d2h, efour
+
+
+def profiled_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(workload, {}).get(kernel)
+    return v
+
+
+# ------------------------------------------------------------- CPU engines
+def cpu_engine(shape, threads):
+    import oracle
+
+    if oracle.ref_available():
+        return oracle.Reference(shape, threads=threads), "reference"
+    return oracle.Restatement(shape, threads=threads), "port"
+
+
+def cpu_setup(wl, threads, seed=0):
+    import oracle
+    from libspimage_b200 import synth
+
+    amp, mask, support, _ = synth.workload(wl["pattern"], seed=0)
+    e, kind = cpu_engine(wl["shape"], threads)
+    name, beta, _ = wl["stages"][0]
+    alg = {"HIO": oracle.HIO, "RAAR": oracle.RAAR, "ER": oracle.ER, "DM": oracle.DIFFMAP}[name]
+    e.set_algorithm(alg, beta=beta, constraints=wl["constraints"])
+    e.add_support_update(oracle.SUP_AREA, wl["period"], wl["blur"], wl["area"])
+    if hasattr(e, "start"):
+        e.start()
+    e.set_amplitudes(amp, mask)
+    e.init_model(oracle.RANDOM_PHASES, seed=seed)
+    e.set_support(support)
+    return e, kind
+
+
+def cpu_baseline(wl, sample_slots):
+    threads = os.cpu_count() or 1
+    e, kind = cpu_setup(wl, threads)
+    t0 = time.perf_counter()
+    e.iterate(sample_slots)
+    dt = time.perf_counter() - t0
+    return {"value": round(sample_slots / dt, 3), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{sample_slots} iteration slots of the first stage ({wl['stages'][0][0]}, incl. "
+                      f"{sample_slots // wl['period']} support updates) of the same workload; FFT threads = cores, "
+                      "FFTW3 API served by the oracle CPU FFT (no libfftw3f on the box)"}
+
+
+def reference_arm(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    wl = WORKLOADS[args.workload]
+    threads = os.cpu_count() or 1
+    e, kind = cpu_setup(wl, threads)
+    sample = args.cpu_sample_slots
+    for _ in range(args.warmup):
+        e.iterate(max(1, sample // 10))
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e.iterate(sample)
+        times.append(time.perf_counter() - t0)
+    total = float(sum(times))
+    value = args.steps * sample / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl["desc"], "shape": list(wl["shape"]),
+                   "step": f"bounded sample: {sample} iteration slots of the first stage per step"},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{sample} iteration slots per step, FFT threads = cores, FFTW3 API served by "
+                                   "the oracle CPU FFT (no libfftw3f on the box)"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="raar1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-sample-slots", type=int, default=300)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -147,6 +147,14 @@ int sp_support_array_update(SpSupportArray *array, SpPhaser *ph);
 /* Not in the reference: message of the last device error seen by this
  * library (the reference calls exit()/abort() on device errors instead). */
 const char *sp_phaser_last_error(void);
+/* Not in the reference: run this phaser's device work on the caller's
+ * cudaStream_t (NULL = the phaser's own stream), so a host framework can
+ * order and time it with its own events.  Returns 0 or -8. */
+int sp_phaser_set_cuda_stream(SpPhaser *ph, void *stream);
+/* Not in the reference: the phaser's device context (spb_ctx *, see
+ * spimage/spb_device.h), created on first use; NULL before the dimensions
+ * are known. */
+void *sp_phaser_device_context(SpPhaser *ph);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,21 @@ int spb_device_count(void);
 int spb_ctx_create(spb_ctx **ctx, int nx, int ny, int nz);
 void spb_ctx_destroy(spb_ctx *ctx);
 int spb_ctx_synchronize(spb_ctx *ctx);
+/* Enqueue this context's work on `stream` (a cudaStream_t of the caller, e.g.
+ * a framework's stream); NULL returns to the context's own stream.  No
+ * reference counterpart (the reference uses the legacy default stream). */
+int spb_ctx_set_stream(spb_ctx *ctx, void *stream);
+
+/* Per-kernel timing with CUDA events recorded around every launch on the
+ * context's stream (no reference counterpart).  Kinds are the pass kernels
+ * named by spb_kernel_name(kind), 0 <= kind < SPB_KERNEL_KINDS. */
+enum { SPB_KERNEL_KINDS = 20 };
+int spb_ctx_profile(spb_ctx *ctx, int enable);
+/* Number of kernels this context has enqueued so far (graph replays count
+ * every kernel node). */
+long long spb_ctx_launch_count(spb_ctx *ctx);
+int spb_ctx_profile_read(spb_ctx *ctx, int kind, long long *launches, double *total_ms);
+const char *spb_kernel_name(int kind);
 
 /* Host -> device copies of the phaser inputs (src/phasing.c:189-363). */
 int spb_ctx_set_amplitudes(spb_ctx *ctx, const float *amp);

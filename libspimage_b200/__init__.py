@@ -132,6 +132,12 @@ def load():
         "sp_image_fftw3": (_IMG, [_IMG]),
         "sp_image_ifftw3": (_IMG, [_IMG]),
         "sp_gaussian_blur": (_IMG, [_IMG, C.c_float]),
+        "sp_phaser_set_cuda_stream": (C.c_int, [_PH, _vp]),
+        "sp_phaser_device_context": (_vp, [_PH]),
+        "spb_ctx_profile": (C.c_int, [_vp, C.c_int]),
+        "spb_ctx_profile_read": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
+        "spb_kernel_name": (C.c_char_p, [C.c_int]),
+        "spb_ctx_launch_count": (C.c_longlong, [_vp]),
         "spb_error_string": (C.c_char_p, []),
         "spb_device_count": (C.c_int, []),
         "spb_fft_host": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _fp, _fp]),
@@ -378,6 +384,29 @@ class Phaser:
 
     def support_fraction(self):
         return float(self.lib.sp_phaser_support_fraction(self.ph))
+
+    # -- extensions: caller stream and per-kernel timing --
+    def set_stream(self, stream_handle):
+        _check(self.lib.sp_phaser_set_cuda_stream(self.ph, stream_handle), "sp_phaser_set_cuda_stream")
+
+    def profile(self, enable):
+        ctx = self.lib.sp_phaser_device_context(self.ph)
+        _check(self.lib.spb_ctx_profile(ctx, 1 if enable else 0), "spb_ctx_profile")
+
+    def launch_count(self):
+        return int(self.lib.spb_ctx_launch_count(self.lib.sp_phaser_device_context(self.ph)))
+
+    def kernel_times(self):
+        """{kernel name: (launches, total ms)} since profiling was enabled."""
+        ctx = self.lib.sp_phaser_device_context(self.ph)
+        out = {}
+        for k in range(20):
+            n = C.c_longlong()
+            ms = C.c_double()
+            _check(self.lib.spb_ctx_profile_read(ctx, k, C.byref(n), C.byref(ms)), "spb_ctx_profile_read")
+            if n.value:
+                out[self.lib.spb_kernel_name(k).decode()] = (int(n.value), float(ms.value))
+        return out
 
 
 # ---- one-shot device entry points (numpy in, numpy out) ----

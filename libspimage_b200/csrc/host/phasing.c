@@ -445,8 +445,8 @@ int sp_phaser_init_model(SpPhaser *ph, const Image *user_model, int flags) {
   }
   if (!rc && (flags & SpModelMaskedOutZeroed)) rc = spb_ctx_mask_out_unmeasured(ctx);
   if (rc) return dev_error("init model");
+  /* host copy is fetched on the first sp_phaser_model() (model_iteration -1) */
   ph->model = sp_image_alloc(ph->nx, ph->ny, ph->nz);
-  if (spb_ctx_get_image(ctx, SPB_G1, (float *)ph->model->image->data)) return dev_error("download model");
   ph->model->phased = 1;
   ph->model_iteration = -1;
   ph->model_change = sp_image_alloc(ph->nx, ph->ny, ph->nz);
@@ -569,6 +569,17 @@ real sp_phaser_support_fraction(SpPhaser *ph) {
   long long c = 0;
   if (spb_ctx_support_count(state(ph)->ctx, &c)) return dev_error("support fraction");
   return (real)c / (real)ph->image_size;
+}
+
+int sp_phaser_set_cuda_stream(SpPhaser *ph, void *stream) {
+  if (ensure_ctx(ph)) return -8;
+  if (spb_ctx_set_stream(state(ph)->ctx, stream)) return dev_error("set stream");
+  return 0;
+}
+
+void *sp_phaser_device_context(SpPhaser *ph) {
+  if (!ph || ensure_ctx(ph)) return NULL;
+  return state(ph)->ctx;
 }
 
 /* -------------------------------------------- hooks for support_update.c */

@@ -85,9 +85,21 @@ int make_axis(Axis &ax, int n) {
     const double ang = (2.0 * 3.14159265358979323846 * (double)i) / (double)n;
     h[i] = make_float2((float)cos(ang), (float)(-sin(ang)));
   }
-  CK(cudaMalloc(&ax.tw, sizeof(float2) * (size_t)n));
+  // per-stage copy of the twiddles used by stage s: [m-1][k] = W_n^(m*k*n/(Ns*R))
+  std::vector<float2> st;
+  int ns_ = 1;
+  for (int s = 0; s < ns; s++) {
+    const int r = radix[s], tstep = n / (ns_ * r);
+    for (int m = 1; m < r; m++)
+      for (int k = 0; k < ns_; k++) st.push_back(h[(size_t)m * k * tstep]);
+    ns_ *= r;
+  }
+  if (st.empty()) st.push_back(make_float2(1.0f, 0.0f));
+  CK(cudaMalloc(&ax.tw, sizeof(float2) * ((size_t)n + st.size())));
   CK(cudaMemcpy(ax.tw, h.data(), sizeof(float2) * (size_t)n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ax.tw + n, st.data(), sizeof(float2) * st.size(), cudaMemcpyHostToDevice));
   ax.lp.tw = ax.tw;
+  ax.lp.stw = ax.tw + n;
   return 0;
 }
 
@@ -97,10 +109,37 @@ const int kMaxAxis = 8192;
 
 }  // namespace
 
+// iterations per captured graph (even: the iterate buffers return to their roles)
+const int kGraphIters = 16;
+const int kMaxGraphs = 8;
+// iterations whose beta values one call can stage on the device
+const int kBetaCap = 1 << 16;
+
+struct GraphEntry {
+  bool used = false;
+  int alg = 0, constraints = 0, objective = 0;
+  float gamma1 = 0.0f, gamma2 = 0.0f;
+  int parity = 0;
+  long long nodes = 0;  // kernel launches per replay
+  cudaGraphExec_t exec = nullptr;
+};
+
+struct KernelProfile {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;  // pairs (start, stop) per launch
+  std::vector<int> kind;
+  size_t used = 0;
+  long long launches[SPB_KERNEL_KINDS] = {};
+  double ms[SPB_KERNEL_KINDS] = {};
+};
+
 struct spb_ctx {
   int nx = 0, ny = 0, nz = 0;
   long long n = 0;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr;      // active stream
+  cudaStream_t own_st = nullptr;  // the context's own stream
+  KernelProfile prof;
+  long long launches = 0;  // kernels enqueued by this context (graph replays count their nodes)
   Axis ax, ay, az;
   float *amp = nullptr, *amin = nullptr, *amax = nullptr;
   float2 *pamp = nullptr;
@@ -109,6 +148,20 @@ struct spb_ctx {
   int cur = 0;
   float2 *X = nullptr, *Y = nullptr, *Xf = nullptr, *Yf = nullptr, *gp = nullptr, *T = nullptr;
   float *absb = nullptr;
+  // line-major operands of the projection pass (lines along the last axis)
+  float *amp_line = nullptr;
+  uint32_t *meas_bits = nullptr;
+  int proj_len = 0, meas_words = 0;
+  long long proj_lines = 0, proj_estride = 0;
+  // CUDA graphs of iteration chunks
+  GraphEntry graphs[kMaxGraphs];
+  int graph_evict = 0;
+  bool use_graphs = true;
+  int warm_alg[5] = {0, 0, 0, 0, 0};
+  float *beta_dev = nullptr, *beta_pinned = nullptr;
+  int beta_cap = 0;
+  int *beta_base = nullptr;
+  cudaEvent_t beta_ev = nullptr;
   SelectState *sel = nullptr;
   double *red = nullptr;
   unsigned long long *cnt = nullptr;
@@ -130,6 +183,9 @@ PassArgs base_args(const spb_ctx *c) {
   a.amp_max = c->amax;
   a.phased_amp = c->pamp;
   a.flags = c->flags;
+  a.amp_line = c->amp_line;
+  a.meas_bits = c->meas_bits;
+  a.meas_words = c->meas_words;
   a.inv_n = (float)(1.0 / (double)c->n);
   a.nx_f = (float)c->nx;
   a.n_f = (float)c->n;
@@ -168,19 +224,58 @@ LinePlan unit_plan() {
   return p;
 }
 
+// ---- optional per-launch event timing
+const int kProfPairs = 4096;
+
+int prof_flush(spb_ctx *c) {
+  KernelProfile &p = c->prof;
+  if (!p.used) return 0;
+  CK(cudaEventSynchronize(p.ev[p.used - 1]));
+  for (size_t i = 0; i < p.used; i += 2) {
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, p.ev[i], p.ev[i + 1]));
+    const int k = p.kind[i / 2];
+    p.ms[k] += ms;
+    p.launches[k] += 1;
+  }
+  p.used = 0;
+  return 0;
+}
+
+int prof_begin(spb_ctx *c) {
+  KernelProfile &p = c->prof;
+  if (!p.on) return 0;
+  if (p.used + 2 > p.ev.size() && prof_flush(c)) return -1;
+  CK(cudaEventRecord(p.ev[p.used], c->st));
+  return 0;
+}
+
+int prof_end(spb_ctx *c, int kind) {
+  KernelProfile &p = c->prof;
+  if (!p.on) return 0;
+  CK(cudaEventRecord(p.ev[p.used + 1], c->st));
+  p.kind[p.used / 2] = kind;
+  p.used += 2;
+  return 0;
+}
+
 int col(spb_ctx *c, int axis, int mode, const float2 *src, float2 *dst, PassArgs a) {
   const LinePlan *pl = nullptr;
   col_geometry(c, axis, a, &pl);
   a.src = src;
   a.dst = dst;
   LinePlan unit = unit_plan();
+  if (prof_begin(c)) return -1;
   CK(launch_col(mode, pl ? *pl : unit, pl ? pl->n : 1, a, c->st));
-  return 0;
+  c->launches++;
+  return prof_end(c, 10 + mode);
 }
 
 int row(spb_ctx *c, int mode, PassArgs a) {
+  if (prof_begin(c)) return -1;
   CK(launch_row(mode, c->ax.lp, a, c->st));
-  return 0;
+  c->launches++;
+  return prof_end(c, mode);
 }
 
 // Non-x axes in transform order (forward: y then z).
@@ -288,11 +383,12 @@ extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) rc = fail("cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
   };
-  cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  cudaError_t e = cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;
     return fail("cudaStreamCreate: %s", cudaGetErrorString(e));
   }
+  c->st = c->own_st;
   alloc((void **)&c->amp, nf);
   alloc((void **)&c->flags, (size_t)c->n);
   alloc((void **)&c->g[0], nc);
@@ -305,6 +401,12 @@ extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
   alloc((void **)&c->sel, sizeof(SelectState));
   alloc((void **)&c->red, sizeof(double) * (4 + 4 * 592));
   alloc((void **)&c->cnt, sizeof(unsigned long long));
+  alloc((void **)&c->beta_base, sizeof(int));
+  alloc((void **)&c->beta_dev, sizeof(float) * kBetaCap);
+  if (!rc && cudaMallocHost(&c->beta_pinned, sizeof(float) * kBetaCap) != cudaSuccess) rc = fail("cudaMallocHost");
+  c->beta_cap = kBetaCap;
+  if (!rc && cudaEventCreateWithFlags(&c->beta_ev, cudaEventDisableTiming) != cudaSuccess) rc = fail("cudaEventCreate");
+  if (!rc && cudaEventRecord(c->beta_ev, c->st) != cudaSuccess) rc = fail("cudaEventRecord");
   if (!rc && make_axis(c->ax, nx)) rc = -1;
   if (!rc && make_axis(c->ay, ny)) rc = -1;
   if (!rc && make_axis(c->az, nz)) rc = -1;
@@ -329,10 +431,18 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
-                  c->gp, c->T, c->absb, c->sel, c->red, c->cnt, c->ax.tw, c->ay.tw, c->az.tw};
+                  c->gp, c->T, c->absb, c->sel, c->red, c->cnt, c->ax.tw, c->ay.tw, c->az.tw,
+                  c->amp_line, c->meas_bits};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  if (c->st) cudaStreamDestroy(c->st);
+  for (auto &e : c->prof.ev) cudaEventDestroy(e);
+  for (auto &g : c->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (c->beta_dev) cudaFree(c->beta_dev);
+  if (c->beta_pinned) cudaFreeHost(c->beta_pinned);
+  if (c->beta_base) cudaFree(c->beta_base);
+  if (c->beta_ev) cudaEventDestroy(c->beta_ev);
+  if (c->own_st) cudaStreamDestroy(c->own_st);
   delete c;
 }
 
@@ -353,8 +463,79 @@ static int download(spb_ctx *c, void *dst, const void *src, size_t bytes) {
   return 0;
 }
 
+namespace spb {
+// amp_line[L*len + i] = amp[i*estride + L]
+__global__ void build_amp_line_kernel(const float *amp, float *amp_line, int len, long long estride,
+                                      long long nlines) {
+  const long long total = nlines * len;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const long long L = k / len, i = k % len;
+    amp_line[k] = amp[i * estride + L];
+  }
+}
+// bit i of line L = measured flag of pixel i*estride + L
+__global__ void build_meas_bits_kernel(const uint8_t *flags, uint32_t *bits, int len, int W, long long estride,
+                                       long long nlines) {
+  const long long total = nlines * W;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const long long L = k / W;
+    const int w = (int)(k % W);
+    uint32_t word = 0;
+    for (int b = 0; b < 32; b++) {
+      const int i = w * 32 + b;
+      if (i < len && (flags[i * estride + L] & FLAG_MEASURED)) word |= 1u << b;
+    }
+    bits[k] = word;
+  }
+}
+}  // namespace spb
+
+// Projection-pass operands in line-major order; only for 2-D/3-D problems
+// whose last axis has a register kernel (power-of-two length).
+static int proj_geometry(spb_ctx *c) {
+  if (c->proj_len) return 1;
+  int len = 0;
+  long long estride = 0;
+  if (c->nz > 1) {
+    len = c->nz;
+    estride = (long long)c->nx * c->ny;
+  } else if (c->ny > 1) {
+    len = c->ny;
+    estride = c->nx;
+  } else {
+    return 0;
+  }
+  if (len < 16 || len > 4096 || (len & (len - 1))) return 0;
+  c->proj_len = len;
+  c->proj_estride = estride;
+  c->proj_lines = estride;
+  c->meas_words = ((len + 127) / 128) * 4;
+  return 1;
+}
+
+static int build_amp_line(spb_ctx *c) {
+  if (!proj_geometry(c)) return 0;
+  if (!c->amp_line) CK(cudaMalloc(&c->amp_line, sizeof(float) * (size_t)c->n));
+  build_amp_line_kernel<<<592, 256, 0, c->st>>>(c->amp, c->amp_line, c->proj_len, c->proj_estride, c->proj_lines);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static int build_meas_bits(spb_ctx *c) {
+  if (!proj_geometry(c)) return 0;
+  const size_t words = (size_t)c->proj_lines * c->meas_words;
+  if (!c->meas_bits) CK(cudaMalloc(&c->meas_bits, sizeof(uint32_t) * words));
+  build_meas_bits_kernel<<<592, 256, 0, c->st>>>(c->flags, c->meas_bits, c->proj_len, c->meas_words,
+                                                 c->proj_estride, c->proj_lines);
+  CK(cudaGetLastError());
+  return 0;
+}
+
 extern "C" int spb_ctx_set_amplitudes(spb_ctx *c, const float *amp) {
-  return upload(c, c->amp, amp, sizeof(float) * (size_t)c->n);
+  if (upload(c, c->amp, amp, sizeof(float) * (size_t)c->n)) return -1;
+  if (build_amp_line(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
 }
 
 extern "C" int spb_ctx_set_margins(spb_ctx *c, const float *amp_min, const float *amp_max) {
@@ -375,6 +556,8 @@ extern "C" int spb_ctx_set_flags(spb_ctx *c, const int *flags) {
   std::vector<uint8_t> h((size_t)c->n);
   for (long long i = 0; i < c->n; i++) h[i] = (uint8_t)(flags[i] & 3);
   if (upload(c, c->flags, h.data(), (size_t)c->n)) return -1;
+  if (build_meas_bits(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
   c->xf_valid = 0;
   return 0;
 }
@@ -439,9 +622,124 @@ extern "C" int spb_ctx_mask_out_unmeasured(spb_ctx *c) {
   return 0;
 }
 
+// One iteration: g0 <- g1 (buffer roles swap), X -> Y (projection pass) ->
+// row pass writing g1 and the next X.  `a` carries the algorithm scalars.
+static int one_iteration(spb_ctx *c, PassArgs a, float2 *gp_out) {
+  c->cur ^= 1;
+  a.g0 = c->g[c->cur ^ 1];
+  a.g1 = c->g[c->cur];
+  a.gp = gp_out;
+  if (middle(c, COL_PROJECT, c->X, c->Y, a)) return -1;
+  if (a.alg == ALG_DM) {
+    if (middle(c, COL_PROJECT_NOFC, c->Xf, c->Yf, a)) return -1;
+    a.src = c->Y;
+    a.src2 = c->Yf;
+    a.dst = c->X;
+    a.dst2 = c->Xf;
+    return row(c, ROW_DM_ITER, a);
+  }
+  a.src = c->Y;
+  a.dst = c->X;
+  return row(c, ROW_ITER, a);
+}
+
+namespace spb {
+__global__ void add_int_kernel(int *p, int v, int set) {
+  if (set) *p = v;
+  else *p += v;
+}
+}  // namespace spb
+
+static bool same_alg(const GraphEntry &g, const spb_alg_desc *d) {
+  return g.alg == d->algorithm && g.constraints == d->constraints && g.objective == d->objective &&
+         g.gamma1 == d->gamma1 && g.gamma2 == d->gamma2;
+}
+
+// Graph of kGraphIters iterations reading beta from the device table at
+// *beta_base + i, followed by beta_base += kGraphIters.  kGraphIters is even,
+// so the iterate buffers return to their roles and the graph can be replayed.
+static int capture_graph(spb_ctx *c, const PassArgs &tmpl, GraphEntry &g) {
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  const int cur0 = c->cur;
+  const long long l0 = c->launches;
+  for (int i = 0; i < kGraphIters && !rc; i++) {
+    PassArgs a = tmpl;
+    a.beta_tab = c->beta_dev;
+    a.beta_base = c->beta_base;
+    a.beta_idx = i;
+    rc = one_iteration(c, a, nullptr);
+  }
+  if (!rc) {
+    add_int_kernel<<<1, 1, 0, c->st>>>(c->beta_base, kGraphIters, 0);
+    if (cudaGetLastError() != cudaSuccess) rc = fail("graph capture: kernel launch failed");
+  }
+  const cudaError_t ee = cudaStreamEndCapture(c->st, &graph);
+  c->cur = cur0;
+  g.nodes = c->launches - l0 + 1;
+  c->launches = l0;
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ee != cudaSuccess) return fail("cudaStreamEndCapture: %s", cudaGetErrorString(ee));
+  const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) return fail("cudaGraphInstantiate: %s", cudaGetErrorString(ie));
+  return 0;
+}
+
+static GraphEntry *find_graph(spb_ctx *c, const spb_alg_desc *d) {
+  for (auto &g : c->graphs)
+    if (g.used && same_alg(g, d) && g.parity == c->cur) return &g;
+  return nullptr;
+}
+
+static GraphEntry *new_graph_slot(spb_ctx *c, const spb_alg_desc *d) {
+  GraphEntry *slot = nullptr;
+  for (auto &g : c->graphs)
+    if (!g.used) { slot = &g; break; }
+  if (!slot) {
+    slot = &c->graphs[c->graph_evict];
+    c->graph_evict = (c->graph_evict + 1) % kMaxGraphs;
+    if (slot->exec) cudaGraphExecDestroy(slot->exec);
+  }
+  *slot = GraphEntry();
+  slot->used = true;
+  slot->alg = d->algorithm;
+  slot->constraints = d->constraints;
+  slot->objective = d->objective;
+  slot->gamma1 = d->gamma1;
+  slot->gamma2 = d->gamma2;
+  slot->parity = c->cur;
+  return slot;
+}
+
+// beta values of this call into the device table (pinned staging, reused
+// only after the previous upload has completed).  The table has a fixed
+// capacity (kBetaCap) allocated with the context: captured graphs hold its
+// address.
+static int upload_betas(spb_ctx *c, const float *beta, int n) {
+  if (n > c->beta_cap) return fail("beta table holds %d iterations, %d requested", c->beta_cap, n);
+  CK(cudaEventSynchronize(c->beta_ev));
+  memcpy(c->beta_pinned, beta, sizeof(float) * (size_t)n);
+  CK(cudaMemcpyAsync(c->beta_dev, c->beta_pinned, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaEventRecord(c->beta_ev, c->st));
+  return 0;
+}
+
 extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float *beta, int iterations,
                                int keep_gp) {
   if (iterations <= 0) return 0;
+  if (iterations > c->beta_cap) {
+    // longer runs go through in table-sized pieces; gp only at the very end
+    for (int off = 0; off < iterations; off += c->beta_cap) {
+      const int k = iterations - off < c->beta_cap ? iterations - off : c->beta_cap;
+      if (spb_ctx_iterate(c, alg, beta + off, k, keep_gp && off + k == iterations)) return -1;
+    }
+    return 0;
+  }
   const int A = alg->algorithm;
   if (A < 1 || A > 4) return fail("unknown algorithm %d", A);
   if (alg->objective == 0 && !c->amp) return fail("amplitudes not set");
@@ -462,27 +760,47 @@ extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float 
   a.gamma2 = alg->gamma2;
   a.one_p_g2 = 1 + alg->gamma2;
   a.size_f = (float)(int)c->n;
-  for (int it = 0; it < iterations; it++) {
-    const float b = (A == ALG_ER) ? 0.0f : beta[it];
-    a.beta = b;
-    a.one_m2b = 1 - 2 * b;
-    c->cur ^= 1;
-    a.g0 = c->g[c->cur ^ 1];
-    a.g1 = c->g[c->cur];
-    a.gp = (keep_gp && it == iterations - 1) ? c->gp : nullptr;
-    if (middle(c, COL_PROJECT, c->X, c->Y, a)) return -1;
-    if (A == ALG_DM) {
-      if (middle(c, COL_PROJECT_NOFC, c->Xf, c->Yf, a)) return -1;
-      a.src = c->Y;
-      a.src2 = c->Yf;
-      a.dst = c->X;
-      a.dst2 = c->Xf;
-      if (row(c, ROW_DM_ITER, a)) return -1;
-    } else {
-      a.src = c->Y;
-      a.dst = c->X;
-      if (row(c, ROW_ITER, a)) return -1;
+  // iterations [0, ngraph) by graph replays, the rest launched directly (the
+  // last one stores gp when asked)
+  const int direct_tail = keep_gp ? 1 : 0;
+  int ngraph = 0;
+  if (c->use_graphs && !c->prof.on) ngraph = ((iterations - direct_tail) / kGraphIters) * kGraphIters;
+  int it = 0;
+  if (ngraph > 0) {
+    GraphEntry *g = find_graph(c, alg);
+    if (!g) {
+      // kernels get their launch attributes from one direct iteration first
+      if (!c->warm_alg[A]) {
+        a.beta = (A == ALG_ER) ? 0.0f : beta[0];
+        if (one_iteration(c, a, nullptr)) return -1;
+        c->warm_alg[A] = 1;
+        it = 1;
+        ngraph = ((iterations - it - direct_tail) / kGraphIters) * kGraphIters;
+      }
+      if (ngraph > 0) {
+        g = new_graph_slot(c, alg);
+        if (capture_graph(c, a, *g)) {
+          g->used = false;
+          return -1;
+        }
+      }
     }
+    if (ngraph > 0) {
+      if (upload_betas(c, beta, iterations)) return -1;
+      add_int_kernel<<<1, 1, 0, c->st>>>(c->beta_base, it, 1);
+      CK(cudaGetLastError());
+      c->launches++;
+      for (int k = 0; k < ngraph; k += kGraphIters) {
+        CK(cudaGraphLaunch(g->exec, c->st));
+        c->launches += g->nodes;
+      }
+      it += ngraph;
+    }
+  }
+  for (; it < iterations; it++) {
+    a.beta = (A == ALG_ER) ? 0.0f : beta[it];
+    if (one_iteration(c, a, (keep_gp && it == iterations - 1) ? c->gp : nullptr)) return -1;
+    c->warm_alg[A] = 1;
   }
   if (A != ALG_DM) c->xf_valid = 0;
   return 0;
@@ -525,7 +843,55 @@ static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *ab
 }
 
 static int select_and_mask(spb_ctx *c, const float *absv, long long n, int type, float value, uint8_t *flags) {
-  return select_and_mask_on(c->st, c->sel, absv, n, type, value, flags);
+  if (prof_begin(c)) return -1;
+  if (select_and_mask_on(c->st, c->sel, absv, n, type, value, flags)) return -1;
+  c->launches += (type == SPB_SUPPORT_AREA) ? 10 : 4;
+  return prof_end(c, type == SPB_SUPPORT_AREA ? 16 : 17);
+}
+
+static const char *kKernelNames[SPB_KERNEL_KINDS] = {
+    "row_fwd",        "row_fwd_dephase", "row_inv",     "row_inv_scale", "row_inv_abs",
+    "row_iter",       "row_dm_f1_fwd",   "row_dm_iter", "row_fwd_f32",   "row_fwd_square_f32",
+    "col_fwd",        "col_inv",         "col_project", "col_project_nofc", "col_blur",
+    "col_inv_square", "select_area",     "select_max",  "unused18",      "unused19"};
+
+extern "C" const char *spb_kernel_name(int kind) {
+  return (kind >= 0 && kind < SPB_KERNEL_KINDS) ? kKernelNames[kind] : "";
+}
+
+extern "C" int spb_ctx_profile(spb_ctx *c, int enable) {
+  KernelProfile &p = c->prof;
+  if (enable && p.ev.empty()) {
+    p.ev.resize(2 * kProfPairs);
+    p.kind.resize(kProfPairs);
+    for (auto &e : p.ev) CK(cudaEventCreate(&e));
+  }
+  if (!enable && prof_flush(c)) return -1;
+  p.on = enable != 0;
+  if (enable) {
+    for (int k = 0; k < SPB_KERNEL_KINDS; k++) {
+      p.launches[k] = 0;
+      p.ms[k] = 0;
+    }
+  }
+  return 0;
+}
+
+extern "C" int spb_ctx_profile_read(spb_ctx *c, int kind, long long *launches, double *total_ms) {
+  if (kind < 0 || kind >= SPB_KERNEL_KINDS) return fail("bad kernel kind %d", kind);
+  if (prof_flush(c)) return -1;
+  *launches = c->prof.launches[kind];
+  *total_ms = c->prof.ms[kind];
+  return 0;
+}
+
+extern "C" long long spb_ctx_launch_count(spb_ctx *c) { return c->launches; }
+
+extern "C" int spb_ctx_set_stream(spb_ctx *c, void *stream) {
+  if (prof_flush(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
+  c->st = stream ? (cudaStream_t)stream : c->own_st;
+  return 0;
 }
 
 extern "C" int spb_ctx_support_update(spb_ctx *c, int type, float radius, float value) {

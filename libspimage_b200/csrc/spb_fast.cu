@@ -1,0 +1,423 @@
+// Register-resident pass kernels for power-of-two line lengths 16..4096.
+//
+// Same transform as spb_fft.cuh (canonical radix plan, same butterflies and
+// twiddle values, explicitly rounded arithmetic), organised for throughput:
+// a line of N points is held by T = N/16 threads, 16 points each, in the
+// "natural" layout v[q] = x[t + T*q].  In that layout the inputs of every
+// butterfly of every stage are already in the thread's registers
+// (a[m] = v[j + m*16/R]), so a stage only scatters its outputs to shared
+// memory and reads the natural layout back: nstages-1 shared-memory
+// exchanges per transform, none after the last stage.  Shared memory is
+// padded (index i -> i + i/16, plus a per-line skew in the column kernels) so
+// that every exchange is free of bank conflicts.  Twiddles are read from a
+// per-stage table laid out [stage][m-1][k] (consecutive k for consecutive
+// threads), holding the very same float values as the per-length table.
+#include <math.h>
+
+#include "spb_internal.h"
+#include "spb_pointwise.cuh"
+
+namespace spb {
+namespace reg {
+
+// number of stages of the canonical plan of a power of two (a trailing 2
+// after 16s turns one 16 into 8*4: still one extra stage)
+__host__ __device__ constexpr int plan_len(int n) {
+  int k = 0, m = n;
+  while (m % 16 == 0) { k++; m /= 16; }
+  if (m > 1) k++;
+  return k;
+}
+
+__host__ __device__ constexpr int plan_radix(int n, int s) {
+  int r[16] = {0};
+  int k = 0, m = n, n16 = 0;
+  while (m % 16 == 0) { r[k++] = 16; m /= 16; n16++; }
+  if (m % 8 == 0) { r[k++] = 8; m /= 8; }
+  else if (m % 4 == 0) { r[k++] = 4; m /= 4; }
+  else if (m % 2 == 0) {
+    if (n16 > 0) { r[k - 1] = 8; r[k++] = 4; }
+    else r[k++] = 2;
+    m /= 2;
+  }
+  return r[s];
+}
+
+__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+
+template <int N, int S, int NS, bool INV>
+struct Stages {
+  static __device__ __forceinline__ void run(float2 (&v)[16], float2 *line, int t, const float2 *stw) {
+    constexpr int R = plan_radix(N, S);
+    constexpr int T = N / 16;
+    constexpr int J = 16 / R;
+    constexpr bool LAST = (S == plan_len(N) - 1);
+#pragma unroll
+    for (int j = 0; j < J; j++) {
+      float2 a[R];
+#pragma unroll
+      for (int m = 0; m < R; m++) a[m] = v[j + m * J];
+      const int b = t + T * j;
+      const int k = b & (NS - 1);
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int m = 1; m < R; m++) {
+          float2 w = stw[(m - 1) * NS + k];  // shared-memory stage table
+          if (INV) w.y = -w.y;
+          const float2 p = cmulw(a[m], w.x, w.y);
+          a[m] = k ? p : a[m];
+        }
+      }
+      bfly<R, INV>(a);
+      if constexpr (LAST) {
+#pragma unroll
+        for (int m = 0; m < R; m++) v[j + m * J] = a[m];
+      } else {
+        const int base = (b / NS) * NS * R + k;
+#pragma unroll
+        for (int m = 0; m < R; m++) line[pad(base + m * NS)] = a[m];
+      }
+    }
+    if constexpr (!LAST) {
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] = line[pad(t + T * q)];
+      __syncthreads();
+      Stages<N, S + 1, NS * R, INV>::run(v, line, t, stw + (R - 1) * NS);
+    }
+  }
+};
+
+template <int N, bool INV>
+__device__ __forceinline__ void fft(float2 (&v)[16], float2 *line, int t, const float2 *stw) {
+  Stages<N, 0, 1, INV>::run(v, line, t, stw);
+}
+
+}  // namespace reg
+
+// ------------------------------------------------------ async copy helpers
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// stage-twiddle table of an N-point line into shared memory (N-1 entries)
+template <int N>
+__device__ __forceinline__ void stage_twiddles(float2 *tw_s, const float2 *__restrict__ stw) {
+  for (int i = threadIdx.x; i < N - 1; i += blockDim.x) cp_async8(tw_s + i, stw + i);
+}
+
+// Fourier projection with the amplitude and measured bit already at hand
+__device__ __forceinline__ float2 project_with(float2 G, float amp, bool measured, long long idx, const PassArgs &a,
+                                               bool fourier_constraints) {
+  if (fourier_constraints && (a.constraints & C_CENTROSYM)) G.y = 0.0f;
+  if (!measured) return G;
+  if (a.objective != 0) return a.phased_amp[idx];
+  float m = 1.0f;
+  if (!(a.constraints & C_MARGIN)) {
+    m = __fdiv_rn(amp, cabs_ref(G));
+  } else {
+    const float av = cabs_ref(G);
+    const float lo = a.amp_min[idx], hi = a.amp_max[idx];
+    if (av < lo) m = __fdiv_rn(lo, av);
+    else if (av > hi) m = __fdiv_rn(hi, av);
+  }
+  if (isfinite(m)) return make_float2(fmul(G.x, m), fmul(G.y, m));
+  return make_float2(amp, 0.0f);
+}
+
+// ------------------------------------------------------------ row kernels
+// Shared memory: [twiddles N][LPB exchange lines of N+N/16]
+//                (ROW_ITER) [LPB rows of g0][LPB rows of flags]
+template <int N, int MODE>
+__global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 *__restrict__ stw, int nrows) {
+  constexpr int T = N / 16;
+  constexpr int S = N + N / 16;
+  extern __shared__ __align__(16) float2 sm[];
+  const int lpb = blockDim.x / T;
+  const int lr = threadIdx.x / T, t = threadIdx.x % T;
+  const int row0 = blockIdx.x * lpb;
+  const int row = row0 + lr;
+  const bool valid = row < nrows;
+  float2 *tw_s = sm;
+  float2 *line = sm + N + lr * S;
+  const size_t base = (size_t)row * N + t;
+  stage_twiddles<N>(tw_s, stw);
+  float2 *g0_s = sm + N + lpb * S;
+  uint8_t *fl_s = reinterpret_cast<uint8_t *>(g0_s + lpb * N);
+  if constexpr (MODE == ROW_ITER) {
+    // g0 and flags of this block's rows: contiguous, copied in 16-byte chunks
+    const int vrows = min(lpb, nrows - row0);
+    const float2 *g0src = a.g0 + (size_t)row0 * N;
+    const int nchunk = vrows * N / 2;
+    for (int c = threadIdx.x; c < nchunk; c += blockDim.x) cp_async16(g0_s + 2 * c, g0src + 2 * c);
+    const uint8_t *fsrc = a.flags + (size_t)row0 * N;
+    const int fchunk = vrows * N / 16;
+    for (int c = threadIdx.x; c < fchunk; c += blockDim.x) cp_async16(fl_s + 16 * c, fsrc + 16 * c);
+  }
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    float2 x = make_float2(0.0f, 0.0f);
+    if (valid) {
+      const size_t idx = base + T * q;
+      if constexpr (MODE == ROW_FWD_DEPHASE) x = make_float2(cabs_ref(a.src[idx]), 0.0f);
+      else if constexpr (MODE == ROW_FWD_F32) x = make_float2(a.f32src[idx], 0.0f);
+      else if constexpr (MODE == ROW_FWD_SQUARE_F32) {
+        const float s = a.f32src[idx];
+        x = make_float2(fmul(s, s), 0.0f);
+      } else x = a.src[idx];
+    }
+    v[q] = x;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if constexpr (MODE == ROW_FWD || MODE == ROW_FWD_DEPHASE || MODE == ROW_FWD_F32 || MODE == ROW_FWD_SQUARE_F32) {
+    reg::fft<N, false>(v, line, t, tw_s);
+    if (valid)
+#pragma unroll
+      for (int q = 0; q < 16; q++) a.dst[base + T * q] = v[q];
+  } else if constexpr (MODE == ROW_INV || MODE == ROW_INV_SCALE || MODE == ROW_INV_ABS) {
+    reg::fft<N, true>(v, line, t, tw_s);
+    if (valid)
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        if constexpr (MODE == ROW_INV) a.dst[base + T * q] = v[q];
+        else if constexpr (MODE == ROW_INV_SCALE) a.dst[base + T * q] = scale_cmul_dev(v[q], a.inv_n);
+        else a.absout[base + T * q] = cabs_ref(v[q]);
+      }
+  } else if constexpr (MODE == ROW_ITER) {
+    const float beta = iter_beta(a);
+    const float one_m2b = fsub(1.0f, fmul(2.0f, beta));  // 1 - 2*beta in float, as the reference
+    reg::fft<N, true>(v, line, t, tw_s);
+    const float2 *g0r = g0_s + lr * N + t;
+    const uint8_t *flr = fl_s + lr * N + t;
+    float2 *gp = a.gp;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      float2 g = make_float2(0.0f, 0.0f);
+      if (valid) {
+        const float2 gpv = scale_cmul_dev(v[q], a.inv_n);
+        if (gp) gp[base + T * q] = gpv;
+        const uint8_t f = flr[T * q];
+        if (f & FLAG_INSIDE) {
+          g = gpv;
+        } else if (a.alg == ALG_HIO) {
+          const float2 g0 = g0r[T * q];
+          g = make_float2(fsub(g0.x, fmul(gpv.x, beta)), fsub(g0.y, fmul(gpv.y, beta)));
+        } else if (a.alg == ALG_RAAR) {
+          const float2 g0 = g0r[T * q];
+          g = make_float2(fadd(fmul(gpv.x, one_m2b), fmul(g0.x, beta)),
+                          fadd(fmul(gpv.y, one_m2b), fmul(g0.y, beta)));
+        }
+        g = apply_constraints(g, f, a.constraints);
+        a.g1[base + T * q] = g;
+      }
+      v[q] = g;
+    }
+    reg::fft<N, false>(v, line, t, tw_s);
+    if (valid)
+#pragma unroll
+      for (int q = 0; q < 16; q++) a.dst[base + T * q] = v[q];
+  }
+}
+
+// --------------------------------------------------------- column kernels
+// Shared memory: [twiddles N][C exchange lines of S]
+//                (projection with line-major operands) [C lines of amp][C lines of measured bits]
+template <int N, int MODE, int C, bool PREFETCH>
+__global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 *__restrict__ stw) {
+  constexpr int T = N / 16;
+  constexpr int S = N + N / 16 + (C > 1 ? 16 / C : 0);
+  extern __shared__ __align__(16) float2 sm[];
+  const int c = threadIdx.x % C, t = threadIdx.x / C;
+  const int col0 = blockIdx.x * C;
+  const int col = col0 + c;
+  const bool valid = col < a.ncols;
+  float2 *tw_s = sm;
+  float2 *line = sm + N + c * S;
+  float *amp_s = reinterpret_cast<float *>(sm + N + C * S);
+  uint32_t *meas_s = reinterpret_cast<uint32_t *>(amp_s + C * N);
+  const int W = a.meas_words;
+  stage_twiddles<N>(tw_s, stw);
+  if constexpr (PREFETCH) {
+    const int vl = min(C, a.ncols - col0);
+    const float *asrc = a.amp_line + (size_t)col0 * N;
+    for (int k = threadIdx.x; k < vl * N / 4; k += blockDim.x) cp_async16(amp_s + 4 * k, asrc + 4 * k);
+    const uint32_t *msrc = a.meas_bits + (size_t)col0 * W;
+    for (int k = threadIdx.x; k < vl * W / 4; k += blockDim.x) cp_async16(meas_s + 4 * k, msrc + 4 * k);
+  }
+  const size_t lbase = (size_t)blockIdx.y * a.ostride + col + (size_t)t * a.estride;
+  const size_t qstride = (size_t)T * a.estride;
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    float2 x = make_float2(0.0f, 0.0f);
+    if (valid) {
+      const size_t idx = lbase + q * qstride;
+      if constexpr (MODE == COL_INV_SQUARE_F32) {
+        const float s = a.f32src[idx];
+        x = make_float2(fmul(s, s), 0.0f);
+      } else {
+        x = a.src[idx];
+      }
+    }
+    v[q] = x;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if constexpr (MODE == COL_FWD) {
+    reg::fft<N, false>(v, line, t, tw_s);
+  } else if constexpr (MODE == COL_INV || MODE == COL_INV_SQUARE_F32) {
+    reg::fft<N, true>(v, line, t, tw_s);
+  } else {
+    reg::fft<N, false>(v, line, t, tw_s);
+    if (valid) {
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const size_t idx = lbase + q * qstride;
+        if constexpr (PREFETCH) {
+          const int i = t + T * q;
+          const float amp = amp_s[c * N + i];
+          const bool meas = (meas_s[c * W + (i >> 5)] >> (i & 31)) & 1u;
+          v[q] = project_with(v[q], amp, meas, idx, a, MODE == COL_PROJECT);
+        } else if constexpr (MODE == COL_PROJECT) {
+          v[q] = project(v[q], idx, a, true);
+        } else if constexpr (MODE == COL_PROJECT_NOFC) {
+          v[q] = project(v[q], idx, a, false);
+        } else {
+          v[q] = gauss_mult(v[q], idx, a);
+        }
+      }
+    }
+    reg::fft<N, true>(v, line, t, tw_s);
+  }
+  if (valid)
+#pragma unroll
+    for (int q = 0; q < 16; q++) a.dst[lbase + q * qstride] = v[q];
+}
+
+// ---------------------------------------------------------------- launch
+template <typename K>
+static cudaError_t set_smem(K k, size_t smem, bool &done) {
+  if (done) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) done = true;
+  return e;
+}
+
+template <int N, int MODE>
+static cudaError_t row_fast_launch(const LinePlan &px, const PassArgs &a, cudaStream_t st) {
+  constexpr int T = N / 16;
+  constexpr int LPB = (256 / T) > 0 ? (256 / T) : 1;
+  const long long nrows = a.n / N;
+  size_t smem = (size_t)(N + LPB * (N + N / 16)) * sizeof(float2);
+  if (MODE == ROW_ITER) smem += (size_t)LPB * N * (sizeof(float2) + 1);
+  auto k = row_fast_kernel<N, MODE>;
+  static bool done = false;
+  cudaError_t e = set_smem(k, smem, done);
+  if (e != cudaSuccess) return e;
+  const long long grid = (nrows + LPB - 1) / LPB;
+  k<<<(unsigned)grid, LPB * T, smem, st>>>(a, px.stw, (int)nrows);
+  return cudaGetLastError();
+}
+
+template <int N>
+__host__ __device__ static constexpr int col_width() {
+  return N >= 2048 ? (4096 / N) : (N >= 512 ? 4 : (N >= 256 ? 8 : 16));
+}
+
+template <int N, int MODE, bool PREFETCH>
+static cudaError_t col_fast_launch_p(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+  constexpr int C = col_width<N>();
+  constexpr int T = N / 16;
+  size_t smem = (size_t)(N + C * (N + N / 16 + (C > 1 ? 16 / C : 0))) * sizeof(float2);
+  if (PREFETCH) smem += (size_t)C * N * sizeof(float) + (size_t)C * a.meas_words * sizeof(uint32_t);
+  auto k = col_fast_kernel<N, MODE, C, PREFETCH>;
+  static bool done = false;
+  static size_t done_smem = 0;
+  if (smem > done_smem) done = false;
+  cudaError_t e = set_smem(k, smem, done);
+  if (e != cudaSuccess) return e;
+  if (smem > done_smem) done_smem = smem;
+  dim3 grid((a.ncols + C - 1) / C, a.nouter);
+  k<<<grid, C * T, smem, st>>>(a, pl.stw);
+  return cudaGetLastError();
+}
+
+template <int N, int MODE>
+static cudaError_t col_fast_launch(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+  constexpr bool PROJ = (MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC);
+  if (PROJ && a.amp_line && a.meas_bits && (a.meas_words % 4) == 0 && a.nouter == 1)
+    return col_fast_launch_p<N, MODE, PROJ>(pl, a, st);
+  return col_fast_launch_p<N, MODE, false>(pl, a, st);
+}
+
+template <int N>
+static cudaError_t row_fast_mode(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st) {
+  switch (mode) {
+    case ROW_FWD: return row_fast_launch<N, ROW_FWD>(px, a, st);
+    case ROW_FWD_DEPHASE: return row_fast_launch<N, ROW_FWD_DEPHASE>(px, a, st);
+    case ROW_INV: return row_fast_launch<N, ROW_INV>(px, a, st);
+    case ROW_INV_SCALE: return row_fast_launch<N, ROW_INV_SCALE>(px, a, st);
+    case ROW_INV_ABS: return row_fast_launch<N, ROW_INV_ABS>(px, a, st);
+    case ROW_ITER: return row_fast_launch<N, ROW_ITER>(px, a, st);
+    case ROW_FWD_F32: return row_fast_launch<N, ROW_FWD_F32>(px, a, st);
+    case ROW_FWD_SQUARE_F32: return row_fast_launch<N, ROW_FWD_SQUARE_F32>(px, a, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+template <int N>
+static cudaError_t col_fast_mode(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+  switch (mode) {
+    case COL_FWD: return col_fast_launch<N, COL_FWD>(pl, a, st);
+    case COL_INV: return col_fast_launch<N, COL_INV>(pl, a, st);
+    case COL_PROJECT: return col_fast_launch<N, COL_PROJECT>(pl, a, st);
+    case COL_PROJECT_NOFC: return col_fast_launch<N, COL_PROJECT_NOFC>(pl, a, st);
+    case COL_BLUR: return col_fast_launch<N, COL_BLUR>(pl, a, st);
+    case COL_INV_SQUARE_F32: return col_fast_launch<N, COL_INV_SQUARE_F32>(pl, a, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+// Returns cudaErrorNotSupported when no register kernel exists for the line
+// length or mode; the caller then uses the general kernels.
+cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st) {
+  if (!px.stw) return cudaErrorNotSupported;
+  switch (px.n) {
+    case 16: return row_fast_mode<16>(mode, px, a, st);
+    case 32: return row_fast_mode<32>(mode, px, a, st);
+    case 64: return row_fast_mode<64>(mode, px, a, st);
+    case 128: return row_fast_mode<128>(mode, px, a, st);
+    case 256: return row_fast_mode<256>(mode, px, a, st);
+    case 512: return row_fast_mode<512>(mode, px, a, st);
+    case 1024: return row_fast_mode<1024>(mode, px, a, st);
+    case 2048: return row_fast_mode<2048>(mode, px, a, st);
+    case 4096: return row_fast_mode<4096>(mode, px, a, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+  if (!pl.stw) return cudaErrorNotSupported;
+  switch (pl.n) {
+    case 16: return col_fast_mode<16>(mode, pl, a, st);
+    case 32: return col_fast_mode<32>(mode, pl, a, st);
+    case 64: return col_fast_mode<64>(mode, pl, a, st);
+    case 128: return col_fast_mode<128>(mode, pl, a, st);
+    case 256: return col_fast_mode<256>(mode, pl, a, st);
+    case 512: return col_fast_mode<512>(mode, pl, a, st);
+    case 1024: return col_fast_mode<1024>(mode, pl, a, st);
+    case 2048: return col_fast_mode<2048>(mode, pl, a, st);
+    case 4096: return col_fast_mode<4096>(mode, pl, a, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+}  // namespace spb

@@ -22,7 +22,8 @@ struct LinePlan {
   int n;
   int nstages;
   int radix[SPB_MAX_STAGES];
-  const float2 *tw;  // n forward twiddles (device)
+  const float2 *tw;   // n forward twiddles W_n^i (device)
+  const float2 *stw;  // the same values per stage: [stage][m-1][k] = W_n^(m*k*n/(Ns*R)) (device)
 };
 
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }

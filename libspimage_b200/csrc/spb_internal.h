@@ -61,9 +61,19 @@ struct PassArgs {
   const float *amp, *amp_min, *amp_max;
   const float2 *phased_amp;
   const uint8_t *flags;
+  // line-major copies for the projection pass (lines along the last axis):
+  // amp_line[L*len + i] and measured bit i of line L in
+  // meas_bits[L*meas_words + i/32]; null when not built
+  const float *amp_line;
+  const uint32_t *meas_bits;
+  int meas_words;
   // scalars
   int alg, constraints, objective;
   float beta, one_m2b, inv_n;
+  // graph replays read beta from a device table: beta_tab[*beta_base + beta_idx]
+  const float *beta_tab;
+  const int *beta_base;
+  int beta_idx;
   float gamma1, gamma2, one_p_g2, size_f;
   // blur
   double blur_c0;   // -2*pow(pi,2) (host glibc)
@@ -81,7 +91,13 @@ struct SelectState {
   unsigned int maxbits;
 };
 
-// host-side launchers (spb_kernels.cu)
+// register-resident kernels (spb_fast.cu); cudaErrorNotSupported when the
+// line length or mode has none
+cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
+
+// host-side launchers (spb_kernels.cu): register kernels where available,
+// general kernels otherwise
 cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_mask_from_abs(const float *absv, const float *thr_dev, float rel, int use_rel, uint8_t *flags,

@@ -12,72 +12,9 @@
 #include <math.h>
 
 #include "spb_internal.h"
+#include "spb_pointwise.cuh"
 
 namespace spb {
-
-__device__ __forceinline__ float2 scale_cmul_dev(float2 v, float s) {
-  // sp_image_scale: complex multiply by (s, 0)
-  return make_float2(fsub(fmul(v.x, s), fmul(v.y, 0.0f)), fadd(fmul(v.x, 0.0f), fmul(s, v.y)));
-}
-
-__device__ __forceinline__ float2 apply_constraints(float2 g, uint8_t f, int c) {
-  if (f & FLAG_INSIDE) {
-    if (c & C_REAL) {
-      g.y = 0.0f;
-    } else if (c & C_POS_REAL) {
-      if (g.x < 0) g.x = (c & C_FLIP) ? fabsf(g.x) : 0.0f;
-      g.y = 0.0f;
-    } else if (c & C_POS_COMPLEX) {
-      if (g.x < 0) g.x = (c & C_FLIP) ? fabsf(g.x) : 0.0f;
-      if (g.y < 0) g.y = (c & C_FLIP) ? fabsf(g.y) : 0.0f;
-    }
-  }
-  return g;
-}
-
-// Fourier-space projection at pixel idx (src/phasing.c:1061-1109)
-__device__ __forceinline__ float2 project(float2 G, long long idx, const PassArgs &a, bool fourier_constraints) {
-  const uint8_t f = a.flags[idx];
-  if (fourier_constraints && (a.constraints & C_CENTROSYM)) G.y = 0.0f;
-  if (a.objective == 0) {
-    if (f & FLAG_MEASURED) {
-      float m = 1.0f;
-      const float amp = a.amp[idx];
-      if (!(a.constraints & C_MARGIN)) {
-        m = __fdiv_rn(amp, cabs_ref(G));
-      } else {
-        const float av = cabs_ref(G);
-        const float lo = a.amp_min[idx], hi = a.amp_max[idx];
-        if (av < lo) m = __fdiv_rn(lo, av);
-        else if (av > hi) m = __fdiv_rn(hi, av);
-      }
-      if (isfinite(m)) G = make_float2(fmul(G.x, m), fmul(G.y, m));
-      else G = make_float2(amp, 0.0f);
-    }
-  } else {
-    if (f & FLAG_MEASURED) G = a.phased_amp[idx];
-  }
-  return G;
-}
-
-// Fourier-domain Gaussian of sp_gaussian_blur (src/image_filter.c:80-90)
-__device__ __forceinline__ float2 gauss_mult(float2 F, long long idx, const PassArgs &a) {
-  const long long nxy = (long long)a.nx * a.ny;
-  const float z = (float)(idx / nxy);
-  const float y = (float)((idx % nxy) / a.nx);
-  const float x = (float)(idx % a.nx);
-  const float fx = (float)a.nx, fy = (float)a.ny, fz = (float)a.nz;
-  const float dx = (__fsub_rn(fx, x) < x) ? __fsub_rn(fx, x) : x;
-  const float dy = (__fsub_rn(fy, y) < y) ? __fsub_rn(fy, y) : y;
-  const float dz = (__fsub_rn(fz, z) < z) ? __fsub_rn(fz, z) : z;
-  const double s = __dadd_rn(__dadd_rn(__dmul_rn((double)dx, (double)dx), __dmul_rn((double)dy, (double)dy)),
-                             __dmul_rn((double)dz, (double)dz));
-  const float dist = __double2float_rn(__dsqrt_rn(s));
-  const float cr = __fdiv_rn(dist, a.nx_f);
-  const double arg = __dmul_rn(__dmul_rn(a.blur_c0, __dmul_rn((double)cr, (double)cr)), a.blur_r2);
-  const float m = __double2float_rn(__ddiv_rn(exp(arg), (double)a.n_f));
-  return scale_cmul_dev(F, m);
-}
 
 // ---------------------------------------------------------------- row pass
 template <int MODE>
@@ -132,6 +69,8 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
       }
     }
   } else if constexpr (MODE == ROW_ITER) {
+    const float beta = iter_beta(a);
+    const float one_m2b = fsub(1.0f, fmul(2.0f, beta));  // 1 - 2*beta in float, as the reference
     float2 *r = line_fft<true>(A, B, px, 1, t, tpr);
     for (int i = t; i < n; i += tpr) {
       float2 g = make_float2(0.0f, 0.0f);
@@ -144,11 +83,11 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
           g = gp;
         } else if (a.alg == ALG_HIO) {
           const float2 g0 = a.g0[idx];
-          g = make_float2(fsub(g0.x, fmul(gp.x, a.beta)), fsub(g0.y, fmul(gp.y, a.beta)));
+          g = make_float2(fsub(g0.x, fmul(gp.x, beta)), fsub(g0.y, fmul(gp.y, beta)));
         } else if (a.alg == ALG_RAAR) {
           const float2 g0 = a.g0[idx];
-          g = make_float2(fadd(fmul(gp.x, a.one_m2b), fmul(g0.x, a.beta)),
-                          fadd(fmul(gp.y, a.one_m2b), fmul(g0.y, a.beta)));
+          g = make_float2(fadd(fmul(gp.x, one_m2b), fmul(g0.x, beta)),
+                          fadd(fmul(gp.y, one_m2b), fmul(g0.y, beta)));
         }
         g = apply_constraints(g, f, a.constraints);
         a.g1[idx] = g;
@@ -161,6 +100,7 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
     if (valid)
       for (int i = t; i < n; i += tpr) a.dst[base + i] = x[i];
   } else if constexpr (MODE == ROW_DM_ITER) {
+    const float beta = iter_beta(a);
     float2 *rho = line_fft<true>(A, B, px, 1, t, tpr);
     float2 *fr = line_fft<true>(Cb, D, px, 1, t, tpr);
     for (int i = t; i < n; i += tpr) {
@@ -171,13 +111,13 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
         if (a.gp) a.gp[idx] = rv;
         const uint8_t f = a.flags[idx];
         if (f & FLAG_INSIDE) {
-          g.x = fadd(g0.x, fmul(a.beta, fsub(__fdiv_rn(fmul(a.one_p_g2, rv.x), a.size_f), fmul(a.gamma2, g0.x))));
-          g.y = fadd(g0.y, fmul(a.beta, fsub(__fdiv_rn(fmul(a.one_p_g2, rv.y), a.size_f), fmul(a.gamma2, g0.y))));
+          g.x = fadd(g0.x, fmul(beta, fsub(__fdiv_rn(fmul(a.one_p_g2, rv.x), a.size_f), fmul(a.gamma2, g0.x))));
+          g.y = fadd(g0.y, fmul(beta, fsub(__fdiv_rn(fmul(a.one_p_g2, rv.y), a.size_f), fmul(a.gamma2, g0.y))));
         } else {
           g = g0;
         }
-        g.x = fsub(g.x, __fdiv_rn(fmul(a.beta, fv.x), a.size_f));
-        g.y = fsub(g.y, __fdiv_rn(fmul(a.beta, fv.y), a.size_f));
+        g.x = fsub(g.x, __fdiv_rn(fmul(beta, fv.x), a.size_f));
+        g.y = fsub(g.y, __fdiv_rn(fmul(beta, fv.y), a.size_f));
         g = apply_constraints(g, f, a.constraints);
         a.g1[idx] = g;
         f1 = (f & FLAG_INSIDE) ? g : make_float2(fmul(-a.gamma1, g.x), fmul(-a.gamma1, g.y));
@@ -276,6 +216,8 @@ static cudaError_t row_launch(const LinePlan &px, const PassArgs &a, cudaStream_
 }
 
 cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st) {
+  const cudaError_t fe = launch_row_fast(mode, px, a, st);
+  if (fe != cudaErrorNotSupported) return fe;
   switch (mode) {
     case ROW_FWD: return row_launch<ROW_FWD>(px, a, st);
     case ROW_FWD_DEPHASE: return row_launch<ROW_FWD_DEPHASE>(px, a, st);
@@ -311,6 +253,8 @@ static cudaError_t col_launch(const LinePlan &pl, const PassArgs &a, cudaStream_
 
 cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArgs &a, cudaStream_t st) {
   (void)line_len;
+  const cudaError_t fe = launch_col_fast(mode, pl, a, st);
+  if (fe != cudaErrorNotSupported) return fe;
   switch (mode) {
     case COL_FWD: return col_launch<COL_FWD>(pl, a, st);
     case COL_INV: return col_launch<COL_INV>(pl, a, st);
@@ -323,44 +267,77 @@ cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArg
 }
 
 // ------------------------------------------------- support selection kernels
-// Keys are the bit patterns of non-negative floats, which order like the floats.
-__global__ void select_hist_kernel(const float *__restrict__ v, long long n, SelectState *s, int shift, int bits) {
-  __shared__ unsigned int h[2048];
-  const int nb = 1 << bits;
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) h[i] = 0;
+// Exact k-th largest value by most-significant-digit radix select over the
+// float bit patterns (non-negative floats order like their bits): four passes
+// of 8 bits, each a histogram of the keys that match the digits fixed so far.
+// Histograms are kept per warp in shared memory and lanes holding the same
+// digit are combined with a match before the atomic, because the leading
+// digits of |blur| concentrate in a few bins.
+#define SEL_BITS 8
+#define SEL_BINS 256
+__global__ void __launch_bounds__(256) select_hist_kernel(const float *__restrict__ v, long long n, SelectState *s,
+                                                          int shift) {
+  __shared__ unsigned int h[8][SEL_BINS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < 8 * SEL_BINS; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
   const unsigned int prefix = s->prefix, pmask = s->prefix_mask;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const unsigned int key = __float_as_uint(v[i]);
-    if ((key & pmask) == prefix) atomicAdd(&h[(key >> shift) & (nb - 1)], 1u);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long start = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long rounds = (n + stride - 1) / stride;
+  for (long long r = 0; r < rounds; r++) {
+    const long long i = start + r * stride;
+    int digit = -1;
+    if (i < n) {
+      const unsigned int key = __float_as_uint(v[i]);
+      if ((key & pmask) == prefix) digit = (int)((key >> shift) & (SEL_BINS - 1));
+    }
+    const unsigned int peers = __match_any_sync(0xffffffffu, digit);
+    if (digit >= 0 && lane == __ffs(peers) - 1) atomicAdd(&h[warp][digit], (unsigned)__popc(peers));
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < nb; i += blockDim.x)
-    if (h[i]) atomicAdd(&s->hist[i], h[i]);
+  for (int d = threadIdx.x; d < SEL_BINS; d += blockDim.x) {
+    unsigned int c = 0;
+    for (int w = 0; w < 8; w++) c += h[w][d];
+    if (c) atomicAdd(&s->hist[d], c);
+  }
 }
 
-// one block: find the digit holding the rank-th largest key, narrow the prefix
-__global__ void select_pick_kernel(SelectState *s, int shift, int bits, int last) {
-  __shared__ unsigned long long csum[2048];
-  const int nb = 1 << bits;
-  // inclusive suffix sums (counts of digits >= d), computed per thread by a simple loop
-  for (int d = threadIdx.x; d < nb; d += blockDim.x) csum[d] = s->hist[d];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long cum = 0;
-    const unsigned long long rank = s->rank;
-    int pick = 0;
-    for (int d = nb - 1; d >= 0; d--) {
-      const unsigned long long c = csum[d];
-      if (cum + c > rank) { pick = d; s->rank = rank - cum; break; }
-      cum += c;
+// one warp: find the digit holding the rank-th largest key, narrow the prefix
+__global__ void select_pick_kernel(SelectState *s, int shift, int last) {
+  const int lane = threadIdx.x;
+  // lane l owns digits [8l, 8l+8); counts of keys with a larger digit come from a suffix scan
+  unsigned long long own = 0;
+  unsigned int c[8];
+  for (int j = 0; j < 8; j++) {
+    c[j] = s->hist[lane * 8 + j];
+    own += c[j];
+  }
+  unsigned long long above = 0;  // keys whose digit is owned by a higher lane
+  for (int l = 31; l > 0; l--) {
+    const unsigned long long x = __shfl_sync(0xffffffffu, own, l);
+    if (l > lane) above += x;
+  }
+  const unsigned long long rank = s->rank;
+  unsigned long long cum = above;
+  int pick = -1;
+  unsigned long long newrank = 0;
+  for (int j = 7; j >= 0; j--) {
+    if (pick < 0 && cum + c[j] > rank && cum <= rank) {
+      pick = lane * 8 + j;
+      newrank = rank - cum;
     }
+    cum += c[j];
+  }
+  __syncwarp();
+  if (pick >= 0) {
     s->prefix |= ((unsigned int)pick) << shift;
-    s->prefix_mask |= ((unsigned int)(nb - 1)) << shift;
+    s->prefix_mask |= ((unsigned int)(SEL_BINS - 1)) << shift;
+    s->rank = newrank;
     if (last) s->result = __uint_as_float(s->prefix);
   }
-  __syncthreads();
-  for (int d = threadIdx.x; d < nb; d += blockDim.x) s->hist[d] = 0;
+  __syncwarp();
+  for (int j = 0; j < 8; j++) s->hist[lane * 8 + j] = 0;
 }
 
 __global__ void select_init_kernel(SelectState *s, unsigned long long rank) {
@@ -376,12 +353,12 @@ __global__ void select_init_kernel(SelectState *s, unsigned long long rank) {
 cudaError_t launch_select_kth_desc(const float *absv, long long n, long long k, SelectState *state,
                                    cudaStream_t st) {
   select_init_kernel<<<1, 256, 0, st>>>(state, (unsigned long long)k);
-  const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
   long long blocks = (n + 255) / 256;
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  for (int p = 0; p < 3; p++) {
-    select_hist_kernel<<<(unsigned)blocks, 256, 0, st>>>(absv, n, state, shifts[p], widths[p]);
-    select_pick_kernel<<<1, 256, 0, st>>>(state, shifts[p], widths[p], p == 2);
+  if (blocks > 148 * 4) blocks = 148 * 4;
+  for (int p = 0; p < 4; p++) {
+    const int shift = 24 - SEL_BITS * p;
+    select_hist_kernel<<<(unsigned)blocks, 256, 0, st>>>(absv, n, state, shift);
+    select_pick_kernel<<<1, 32, 0, st>>>(state, shift, p == 3);
   }
   return cudaGetLastError();
 }

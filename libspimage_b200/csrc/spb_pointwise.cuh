@@ -1,0 +1,78 @@
+// Pointwise steps of the phasing passes, shared by the general and the
+// register-resident kernels.  Each follows the reference engine's float
+// operation order with explicitly rounded intrinsics.
+#pragma once
+#include "spb_internal.h"
+
+namespace spb {
+
+__device__ __forceinline__ float2 scale_cmul_dev(float2 v, float s) {
+  // sp_image_scale: complex multiply by (s, 0)
+  return make_float2(fsub(fmul(v.x, s), fmul(v.y, 0.0f)), fadd(fmul(v.x, 0.0f), fmul(s, v.y)));
+}
+
+// beta of this iteration: kernel argument, or the device table during graph replays
+__device__ __forceinline__ float iter_beta(const PassArgs &a) {
+  return a.beta_tab ? a.beta_tab[*a.beta_base + a.beta_idx] : a.beta;
+}
+
+__device__ __forceinline__ float2 apply_constraints(float2 g, uint8_t f, int c) {
+  if (f & FLAG_INSIDE) {
+    if (c & C_REAL) {
+      g.y = 0.0f;
+    } else if (c & C_POS_REAL) {
+      if (g.x < 0) g.x = (c & C_FLIP) ? fabsf(g.x) : 0.0f;
+      g.y = 0.0f;
+    } else if (c & C_POS_COMPLEX) {
+      if (g.x < 0) g.x = (c & C_FLIP) ? fabsf(g.x) : 0.0f;
+      if (g.y < 0) g.y = (c & C_FLIP) ? fabsf(g.y) : 0.0f;
+    }
+  }
+  return g;
+}
+
+// Fourier-space projection at pixel idx (src/phasing.c:1061-1109)
+__device__ __forceinline__ float2 project(float2 G, long long idx, const PassArgs &a, bool fourier_constraints) {
+  const uint8_t f = a.flags[idx];
+  if (fourier_constraints && (a.constraints & C_CENTROSYM)) G.y = 0.0f;
+  if (a.objective == 0) {
+    if (f & FLAG_MEASURED) {
+      float m = 1.0f;
+      const float amp = a.amp[idx];
+      if (!(a.constraints & C_MARGIN)) {
+        m = __fdiv_rn(amp, cabs_ref(G));
+      } else {
+        const float av = cabs_ref(G);
+        const float lo = a.amp_min[idx], hi = a.amp_max[idx];
+        if (av < lo) m = __fdiv_rn(lo, av);
+        else if (av > hi) m = __fdiv_rn(hi, av);
+      }
+      if (isfinite(m)) G = make_float2(fmul(G.x, m), fmul(G.y, m));
+      else G = make_float2(amp, 0.0f);
+    }
+  } else {
+    if (f & FLAG_MEASURED) G = a.phased_amp[idx];
+  }
+  return G;
+}
+
+// Fourier-domain Gaussian of sp_gaussian_blur (src/image_filter.c:80-90)
+__device__ __forceinline__ float2 gauss_mult(float2 F, long long idx, const PassArgs &a) {
+  const long long nxy = (long long)a.nx * a.ny;
+  const float z = (float)(idx / nxy);
+  const float y = (float)((idx % nxy) / a.nx);
+  const float x = (float)(idx % a.nx);
+  const float fx = (float)a.nx, fy = (float)a.ny, fz = (float)a.nz;
+  const float dx = (__fsub_rn(fx, x) < x) ? __fsub_rn(fx, x) : x;
+  const float dy = (__fsub_rn(fy, y) < y) ? __fsub_rn(fy, y) : y;
+  const float dz = (__fsub_rn(fz, z) < z) ? __fsub_rn(fz, z) : z;
+  const double s = __dadd_rn(__dadd_rn(__dmul_rn((double)dx, (double)dx), __dmul_rn((double)dy, (double)dy)),
+                             __dmul_rn((double)dz, (double)dz));
+  const float dist = __double2float_rn(__dsqrt_rn(s));
+  const float cr = __fdiv_rn(dist, a.nx_f);
+  const double arg = __dmul_rn(__dmul_rn(a.blur_c0, __dmul_rn((double)cr, (double)cr)), a.blur_r2);
+  const float m = __double2float_rn(__ddiv_rn(exp(arg), (double)a.n_f));
+  return scale_cmul_dev(F, m);
+}
+
+}  // namespace spb

@@ -18,6 +18,7 @@ def setup(engine, shape, alg, sup=None, constraints=2, beta=0.9, seed=3, pattern
     if hasattr(engine, "start"):
         engine.start()
     engine.set_amplitudes(amp, mask)
+    engine.amplitudes_np = amp
     rc = engine.init_model(init_flags, seed=seed)
     assert rc == 0
     if patterson is not None:
