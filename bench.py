@@ -169,10 +169,11 @@ def gpu_arm(args):
     import libspimage_b200 as L
     from libspimage_b200 import synth
 
-    world, rank, local = dist_setup()
+    from libspimage_b200 import replicas
+
+    world, rank, local = replicas.dist_env()
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    replicas.init("nccl", timeout_s=300)
     wl = WORKLOADS[args.workload]
     n = int(np.prod(wl["shape"]))
     amp, mask, support, _ = synth.workload(wl["pattern"], seed=0)
@@ -220,11 +221,7 @@ def gpu_arm(args):
     torch.cuda.synchronize()
     ktimes = ph.kernel_times()
     ph.profile(False)
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = replicas.max_over_ranks(float(sum(step_ms)), device="cuda")
     slots = slots_per_step(wl)
     value = world * args.steps * slots / (total_ms / 1e3)
 
@@ -276,6 +273,8 @@ def e2e_run(args, L, wl, amp, mask, support, rank, world, torch, dist):
     """Full user flow per step with host inputs; wall clock, max over ranks."""
     import ctypes as C
 
+    from libspimage_b200 import replicas
+
     n = int(np.prod(wl["shape"]))
     ph = L.Phaser(wl["shape"])
     handles = []
@@ -317,11 +316,7 @@ def e2e_run(args, L, wl, amp, mask, support, rank, world, torch, dist):
         t0 = time.perf_counter()
         efour = one(rank * 1000 + k)
         times.append(time.perf_counter() - t0)
-    total = float(sum(times))
-    if world > 1:
-        t = torch.tensor([total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = replicas.max_over_ranks(float(sum(times)), device="cuda")
     for ptr in pinned:
         cudart.cudaHostUnregister(ptr)
     ph.close()

@@ -110,6 +110,7 @@ def _load_restatement():
         lib.spo_area_threshold.restype = C.c_float
         lib.spo_area_threshold.argtypes = [C.c_long, _fp, C.c_float]
         lib.spo_fft.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _fp, _fp]
+        lib.spo_module_projection.argtypes = [C.c_long, _fp, _fp, _ip, C.c_int]
         _libs["rs"] = lib
         return lib
 
@@ -474,6 +475,16 @@ def area_threshold(blur, area):
     lib = _load_restatement()
     a = _c64(blur).ravel()
     return float(lib.spo_area_threshold(a.size, _ptr(a), area))
+
+
+def module_projection(G, amp, flags, constraints=0):
+    """The Fourier-modulus projection alone (src/phasing.c:1070-1100)."""
+    lib = _load_restatement()
+    g = _c64(G).ravel().copy()
+    a = _f32(amp).ravel()
+    f = np.ascontiguousarray(flags, dtype=np.int32).ravel()
+    lib.spo_module_projection(g.size, _ptr(g), _ptr(a), _ptr(f, _ip), constraints)
+    return g.reshape(np.shape(G))
 
 
 def bezier(smap, x):

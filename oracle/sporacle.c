@@ -331,6 +331,16 @@ static void module_projection(spo_phaser *ph, spfft_cpx *G, int c) {
   }
 }
 
+/* the projection alone on caller arrays (element-level tests) */
+void spo_module_projection(long n, spfft_cpx *G, const float *amp, const int *flags, int constraints) {
+  spo_phaser tmp;
+  memset(&tmp, 0, sizeof(tmp));
+  tmp.n = n;
+  tmp.amp = (float *)amp;
+  tmp.flags = (int *)flags;
+  module_projection(&tmp, G, constraints & ~SPO_MARGIN);
+}
+
 static void phased_amp_projection(spo_phaser *ph, spfft_cpx *G) {
   for (long i = 0; i < ph->n; i++)
     if (ph->flags[i] & SPO_MEASURED) G[i] = ph->phased_amp[i];

@@ -61,6 +61,7 @@ float spo_dm_gamma(spo_phaser *ph, int which);
 /* building blocks, exposed for element-level tests */
 void spo_gaussian_blur(int nx, int ny, int nz, const spfft_cpx *in, float radius, spfft_cpx *out);
 float spo_area_threshold(long n, const spfft_cpx *blur, float area);
+void spo_module_projection(long n, spfft_cpx *G, const float *amp, const int *flags, int constraints);
 void spo_fft(int nx, int ny, int nz, int sign, const spfft_cpx *in, spfft_cpx *out);
 
 #ifdef __cplusplus
