@@ -331,13 +331,15 @@ def e2e_run(args, L, wl, amp, mask, support, rank, world, torch, dist):
 
 def profiled_traffic(kernel, workload):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+    p = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        d = json.load(f)
-    v = d.get(workload, {}).get(kernel)
-    return v
+        for line in f:
+            parts = line.split()
+            if len(parts) == 3 and not line.startswith("#") and parts[0] == workload and parts[1] == kernel:
+                return int(parts[2])
+    return None
 
 
 # ------------------------------------------------------------- CPU engines
