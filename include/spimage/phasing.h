@@ -156,6 +156,38 @@ int sp_phaser_set_cuda_stream(SpPhaser *ph, void *stream);
  * are known. */
 void *sp_phaser_device_context(SpPhaser *ph);
 
+/* Not in the reference: batched random starts.  The reference's
+ * Reconstructor.reconstruct_loop (src/_spimage_reconstructor.py:677-740) runs
+ * one reconstruction after another from different random starts; here one
+ * SpPhaser advances `starts` independent reconstructions of the same pattern
+ * together.  Call sp_phaser_set_starts before sp_phaser_init_model (it drops
+ * the device state and the model).  Afterwards every SpPhaser call applies to
+ * all starts: the algorithm, schedules, support updates and host-side edits
+ * of the support are shared, each start keeps its own model and support, and
+ * the single-image accessors (sp_phaser_model, sp_phaser_support,
+ * sp_phaser_efourier, ...) report start 0.  Start b's results are bit for
+ * bit those of a one-start phaser given the same starting model.  Returns 0,
+ * -1 for starts < 1, -8 on a device error. */
+int sp_phaser_set_starts(SpPhaser *ph, int starts);
+int sp_phaser_starts(const SpPhaser *ph);
+/* Starting models drawn per start on the host exactly as sp_phaser_init_model
+ * draws them after sp_srand(seeds[b]) (flags as there, user model not
+ * allowed), so start b reproduces a one-start run seeded with seeds[b]. */
+int sp_phaser_init_models(SpPhaser *ph, int flags, const int *seeds);
+/* Random-phase starting models drawn on the device (Philox4x32-10 keyed by
+ * seeds[b]); for throughput runs that do not need the reference's rand()
+ * stream.  SpModelMaskedOutZeroed may be added to flags. */
+int sp_phaser_init_models_device(SpPhaser *ph, int flags, const unsigned long long *seeds);
+/* Start b's model, support (1 inside, 0 outside) or model before projection
+ * copied into `out` (an image of the phaser's shape). */
+int sp_phaser_start_model(SpPhaser *ph, int start, Image *out);
+int sp_phaser_start_support(SpPhaser *ph, int start, Image *out);
+int sp_phaser_start_model_before_projection(SpPhaser *ph, int start, Image *out);
+/* Per-start metrics into out[starts] (FcFo may be NULL). */
+int sp_phaser_starts_efourier(SpPhaser *ph, real *out, real *FcFo);
+int sp_phaser_starts_ereal(SpPhaser *ph, real *out);
+int sp_phaser_starts_support_fraction(SpPhaser *ph, real *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,6 +97,34 @@ int spb_ctx_efourier_sums(spb_ctx *ctx, double sums[4]);
 int spb_ctx_ereal_sums(spb_ctx *ctx, double sums[2]);
 int spb_ctx_support_count(spb_ctx *ctx, long long *count);
 
+/* Batched starts.  A batch context holds nb independent reconstructions of
+ * ONE pattern (shared amplitudes, margins and measured mask; per-start model,
+ * iterates and support), stacked start-major.  Every call above acts on all
+ * starts at once: set_flags, set_model and model_from_fourier give every
+ * start the same value, iterate advances every start, support_update
+ * thresholds each start's own blurred model, and the single-start getters
+ * read start 0.  This replaces the sequential loop of the reference's
+ * Reconstructor.reconstruct_loop (src/_spimage_reconstructor.py:677-740),
+ * which runs one SpPhaser after another; each start's result is bit-for-bit
+ * the one a single-start context gives for the same start. */
+int spb_ctx_create_batch(spb_ctx **ctx, int nx, int ny, int nz, int nb);
+int spb_ctx_starts(spb_ctx *ctx);
+/* per-start flags; the measured bit must be the same pattern in every start */
+int spb_ctx_set_start_flags(spb_ctx *ctx, int start, const int *flags);
+int spb_ctx_get_start_flags(spb_ctx *ctx, int start, int *flags);
+int spb_ctx_set_start_model(spb_ctx *ctx, int start, const float *model, int reset_others);
+/* fourier holds nb spectra, start-major: g1[b] = IFFT(fourier[b])/N */
+int spb_ctx_models_from_fourier(spb_ctx *ctx, const float *fourier, int reset_others);
+/* g1[b] = IFFT(amp * exp(2 pi i u))/N with u drawn on the device by
+ * Philox4x32-10 keyed by seeds[b] (throughput runs; the host API's
+ * SpModelRandomPhases reproduces the reference's rand() stream instead) */
+int spb_ctx_random_phase_models(spb_ctx *ctx, const unsigned long long *seeds, int reset_others);
+int spb_ctx_get_start_image(spb_ctx *ctx, int start, int which, float *out);
+/* sums[b*4 + k]: efourier {nom, den, FcFo num, FcFo den}, ereal {nom, den, 0, 0} */
+int spb_ctx_batch_efourier_sums(spb_ctx *ctx, double *sums);
+int spb_ctx_batch_ereal_sums(spb_ctx *ctx, double *sums);
+int spb_ctx_batch_support_counts(spb_ctx *ctx, long long *counts);
+
 /* One-shot transforms of host buffers (sp_image_fft/ifft, src/fft.c:53-189,
  * src/fft.cu:7-43; sp_gaussian_blur, src/image_filter.c:80-90).  sign -1 is
  * forward, +1 backward (unnormalised). */

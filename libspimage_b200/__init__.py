@@ -143,6 +143,16 @@ def load():
         "spb_fft_host": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _fp, _fp]),
         "spb_blur_host": (C.c_int, [C.c_int, C.c_int, C.c_int, _fp, C.c_float, _fp]),
         "spb_support_from_blur_host": (C.c_int, [C.c_longlong, _fp, C.c_int, C.c_float, _ip]),
+        "sp_phaser_set_starts": (C.c_int, [_PH, C.c_int]),
+        "sp_phaser_starts": (C.c_int, [_PH]),
+        "sp_phaser_init_models": (C.c_int, [_PH, C.c_int, _ip]),
+        "sp_phaser_init_models_device": (C.c_int, [_PH, C.c_int, C.POINTER(C.c_ulonglong)]),
+        "sp_phaser_start_model": (C.c_int, [_PH, C.c_int, _IMG]),
+        "sp_phaser_start_support": (C.c_int, [_PH, C.c_int, _IMG]),
+        "sp_phaser_start_model_before_projection": (C.c_int, [_PH, C.c_int, _IMG]),
+        "sp_phaser_starts_efourier": (C.c_int, [_PH, _fp, _fp]),
+        "sp_phaser_starts_ereal": (C.c_int, [_PH, _fp]),
+        "sp_phaser_starts_support_fraction": (C.c_int, [_PH, _fp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -384,6 +394,57 @@ class Phaser:
 
     def support_fraction(self):
         return float(self.lib.sp_phaser_support_fraction(self.ph))
+
+    # -- extension: batched random starts of one pattern --
+    def set_starts(self, nb):
+        _check(self.lib.sp_phaser_set_starts(self.ph, int(nb)), "sp_phaser_set_starts")
+
+    @property
+    def starts(self):
+        return int(self.lib.sp_phaser_starts(self.ph))
+
+    def init_models(self, flags, seeds):
+        s = np.ascontiguousarray(seeds, dtype=np.int32)
+        assert s.size == self.starts
+        return self.lib.sp_phaser_init_models(self.ph, flags, _p(s, _ip))
+
+    def init_models_device(self, flags, seeds):
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        assert s.size == self.starts
+        return self.lib.sp_phaser_init_models_device(self.ph, flags, s.ctypes.data_as(C.POINTER(C.c_ulonglong)))
+
+    def _start_image(self, fn, b):
+        img = self._img(np.zeros(self.shape, np.complex64))
+        _check(fn(self.ph, int(b), img), fn.__name__)
+        out = image_data(img, self.shape)
+        self._owned.remove(img)
+        free_image(img)
+        return out
+
+    def start_model(self, b):
+        return self._start_image(self.lib.sp_phaser_start_model, b)
+
+    def start_model_before_projection(self, b):
+        return self._start_image(self.lib.sp_phaser_start_model_before_projection, b)
+
+    def start_support(self, b):
+        return (self._start_image(self.lib.sp_phaser_start_support, b).real != 0).astype(np.int32)
+
+    def starts_efourier(self):
+        e = np.zeros(self.starts, np.float32)
+        f = np.zeros(self.starts, np.float32)
+        _check(self.lib.sp_phaser_starts_efourier(self.ph, _p(e), _p(f)), "sp_phaser_starts_efourier")
+        return e, f
+
+    def starts_ereal(self):
+        e = np.zeros(self.starts, np.float32)
+        _check(self.lib.sp_phaser_starts_ereal(self.ph, _p(e)), "sp_phaser_starts_ereal")
+        return e
+
+    def starts_support_fraction(self):
+        e = np.zeros(self.starts, np.float32)
+        _check(self.lib.sp_phaser_starts_support_fraction(self.ph, _p(e)), "sp_phaser_starts_support_fraction")
+        return e
 
     # -- extensions: caller stream and per-kernel timing --
     def set_stream(self, stream_handle):

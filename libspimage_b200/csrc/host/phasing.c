@@ -18,6 +18,7 @@
 
 typedef struct {
   spb_ctx *ctx;
+  int starts; /* independent reconstructions in the context (0 = 1) */
   int amp_dirty, flags_dirty, margins_dirty, pamp_dirty;
   int flags_dev_newer; /* device flags changed by a support update */
 } dev_state;
@@ -44,7 +45,8 @@ static int ensure_ctx(SpPhaser *ph) {
     snprintf(g_last_err, sizeof(g_last_err), "phaser dimensions are not set");
     return -8;
   }
-  if (spb_ctx_create(&s->ctx, ph->nx, ph->ny, ph->nz)) return dev_error("device context");
+  if (spb_ctx_create_batch(&s->ctx, ph->nx, ph->ny, ph->nz, s->starts > 0 ? s->starts : 1))
+    return dev_error("device context");
   s->amp_dirty = ph->amplitudes != NULL;
   s->flags_dirty = ph->pixel_flags != NULL;
   s->margins_dirty = ph->amplitudes_min != NULL;
@@ -397,6 +399,9 @@ int sp_phaser_set_support_algorithm(SpPhaser *ph, SpSupportArray *alg) {
   return 0;
 }
 
+static int draw_start(SpPhaser *ph, int flags, Image *m);
+static int finish_init_model(SpPhaser *ph, int flags, int rc);
+
 /* phasing.c:606-724 with the CPU engine's semantics: the starting model is
  * derived from the host RNG (glibc rand(), as p_drand48) exactly like the
  * reference CPU engine, then transformed on the GPU. */
@@ -412,44 +417,197 @@ int sp_phaser_init_model(SpPhaser *ph, const Image *user_model, int flags) {
   if (user_model) phaser_check_dimensions(ph, user_model);
   if (sync_to_device(ph)) return -8;
   spb_ctx *ctx = state(ph)->ctx;
-  const int n = ph->image_size;
   int rc = 0;
   if (user_model) {
     rc = spb_ctx_set_model(ctx, (const float *)user_model->image->data, 1);
-  } else if (flags & (SpModelRandomPhases | SpModelZeroPhases)) {
-    Image *tmp = sp_image_alloc(ph->nx, ph->ny, ph->nz);
-    for (int i = 0; i < n; i++) tmp->image->data[i].re = ph->amplitudes->data[i];
-    sp_image_rephase(tmp, (flags & SpModelRandomPhases) ? SP_RANDOM_PHASE : SP_ZERO_PHASE);
-    rc = spb_ctx_model_from_fourier(ctx, (const float *)tmp->image->data, 1);
-    sp_image_free(tmp);
   } else {
-    /* SpModelRandomValues: uniform (re, im) in [-0.5, 0.5) scaled so that the
-     * squared norm matches the amplitudes' (phasing.c:674-690) */
     Image *m = sp_image_alloc(ph->nx, ph->ny, ph->nz);
-    double sum = 0;
-    for (int i = 0; i < n; i++) sum += ph->amplitudes->data[i] * ph->amplitudes->data[i];
-    sum /= n;
-    for (int i = 0; i < n; i++) {
-      /* the reference's sp_cinit(p_drand48()-0.5, p_drand48()-0.5) draws the
-       * imaginary part first under gcc's argument evaluation order */
-      const real im = p_drand48() - 0.5;
-      const real re = p_drand48() - 0.5;
-      m->image->data[i] = sp_cinit(re, im);
-    }
-    double msum = 0;
-    for (int i = 0; i < n; i++) msum += sp_cabs2(m->image->data[i]);
-    const real model_sum = (real)msum;
-    sp_image_scale(m, sqrt(sum / model_sum));
-    rc = spb_ctx_set_model(ctx, (const float *)m->image->data, 1);
+    if (draw_start(ph, flags, m)) rc = spb_ctx_model_from_fourier(ctx, (const float *)m->image->data, 1);
+    else rc = spb_ctx_set_model(ctx, (const float *)m->image->data, 1);
     sp_image_free(m);
   }
-  if (!rc && (flags & SpModelMaskedOutZeroed)) rc = spb_ctx_mask_out_unmeasured(ctx);
+  return finish_init_model(ph, flags, rc);
+}
+
+/* Fills `m` from the host RNG as the reference's CPU engine does for `flags`;
+ * returns 1 when `m` is a Fourier-space start (random or zero phases on the
+ * amplitudes), 0 when it is a real-space model (random values). */
+static int draw_start(SpPhaser *ph, int flags, Image *m) {
+  const int n = ph->image_size;
+  if (flags & (SpModelRandomPhases | SpModelZeroPhases)) {
+    for (int i = 0; i < n; i++) m->image->data[i] = sp_cinit(ph->amplitudes->data[i], 0);
+    sp_image_rephase(m, (flags & SpModelRandomPhases) ? SP_RANDOM_PHASE : SP_ZERO_PHASE);
+    return 1;
+  }
+  /* SpModelRandomValues: uniform (re, im) in [-0.5, 0.5) scaled so that the
+   * squared norm matches the amplitudes' (phasing.c:674-690) */
+  double sum = 0;
+  for (int i = 0; i < n; i++) sum += ph->amplitudes->data[i] * ph->amplitudes->data[i];
+  sum /= n;
+  for (int i = 0; i < n; i++) {
+    /* the reference's sp_cinit(p_drand48()-0.5, p_drand48()-0.5) draws the
+     * imaginary part first under gcc's argument evaluation order */
+    const real im = p_drand48() - 0.5;
+    const real re = p_drand48() - 0.5;
+    m->image->data[i] = sp_cinit(re, im);
+  }
+  double msum = 0;
+  for (int i = 0; i < n; i++) msum += sp_cabs2(m->image->data[i]);
+  const real model_sum = (real)msum;
+  sp_image_scale(m, sqrt(sum / model_sum));
+  return 0;
+}
+
+static int finish_init_model(SpPhaser *ph, int flags, int rc) {
+  if (!rc && (flags & SpModelMaskedOutZeroed)) rc = spb_ctx_mask_out_unmeasured(state(ph)->ctx);
   if (rc) return dev_error("init model");
   /* host copy is fetched on the first sp_phaser_model() (model_iteration -1) */
   ph->model = sp_image_alloc(ph->nx, ph->ny, ph->nz);
   ph->model->phased = 1;
   ph->model_iteration = -1;
   ph->model_change = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  return 0;
+}
+
+static int init_models_check(SpPhaser *ph, int flags) {
+  if (!ph) return -1;
+  if (ph->engine != SpEngineCUDA) {
+    snprintf(g_last_err, sizeof(g_last_err), "sp_phaser_init must succeed before sp_phaser_init_model");
+    return -3;
+  }
+  if (ph->model) { sp_image_free(ph->model); ph->model = NULL; }
+  if (ph->model_change) { sp_image_free(ph->model_change); ph->model_change = NULL; }
+  if (!(flags & (SpModelRandomPhases | SpModelZeroPhases | SpModelRandomValues))) return -3;
+  if (!ph->amplitudes) return -3;
+  if (sync_to_device(ph)) return -8;
+  return 0;
+}
+
+int sp_phaser_init_models(SpPhaser *ph, int flags, const int *seeds) {
+  const int rc0 = init_models_check(ph, flags);
+  if (rc0) return rc0;
+  spb_ctx *ctx = state(ph)->ctx;
+  const int nb = sp_phaser_starts(ph);
+  const size_t n = (size_t)ph->image_size;
+  Image *m = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  int rc = 0;
+  if (flags & (SpModelRandomPhases | SpModelZeroPhases)) {
+    /* nb Fourier-space starts, transformed together on the device */
+    float *all = (float *)malloc(sizeof(float) * 2 * n * (size_t)nb);
+    for (int b = 0; b < nb; b++) {
+      sp_srand(seeds[b]);
+      draw_start(ph, flags, m);
+      memcpy(all + 2 * n * (size_t)b, m->image->data, sizeof(float) * 2 * n);
+    }
+    rc = spb_ctx_models_from_fourier(ctx, all, 1);
+    free(all);
+  } else {
+    for (int b = 0; b < nb && !rc; b++) {
+      sp_srand(seeds[b]);
+      draw_start(ph, flags, m);
+      rc = spb_ctx_set_start_model(ctx, b, (const float *)m->image->data, b == 0);
+    }
+  }
+  sp_image_free(m);
+  return finish_init_model(ph, flags, rc);
+}
+
+int sp_phaser_init_models_device(SpPhaser *ph, int flags, const unsigned long long *seeds) {
+  const int rc0 = init_models_check(ph, flags | SpModelRandomPhases);
+  if (rc0) return rc0;
+  const int rc = spb_ctx_random_phase_models(state(ph)->ctx, seeds, 1);
+  return finish_init_model(ph, flags, rc);
+}
+
+int sp_phaser_starts(const SpPhaser *ph) {
+  const dev_state *s = (const dev_state *)ph->device;
+  return (s && s->starts > 0) ? s->starts : 1;
+}
+
+int sp_phaser_set_starts(SpPhaser *ph, int starts) {
+  if (!ph || starts < 1) return -1;
+  dev_state *s = state(ph);
+  if (s->ctx) {
+    if (sync_flags_to_host(ph)) return -8;
+    spb_ctx_destroy(s->ctx);
+    s->ctx = NULL;
+  }
+  s->starts = starts;
+  s->flags_dev_newer = 0;
+  if (ph->model) { sp_image_free(ph->model); ph->model = NULL; }
+  if (ph->model_change) { sp_image_free(ph->model_change); ph->model_change = NULL; }
+  ph->model_iteration = ph->fmodel_iteration = ph->model_before_projection_iteration = -1;
+  ph->old_model_iteration = ph->support_iteration = -1;
+  return 0;
+}
+
+static int start_image(SpPhaser *ph, int start, Image *out, int which) {
+  if (!out || sp_image_x(out) != ph->nx || sp_image_y(out) != ph->ny || sp_image_z(out) != ph->nz) return -1;
+  if (ensure_ctx(ph)) return -8;
+  if (spb_ctx_get_start_image(state(ph)->ctx, start, which, (float *)out->image->data))
+    return dev_error("download start image");
+  out->phased = 1;
+  return 0;
+}
+
+int sp_phaser_start_model(SpPhaser *ph, int start, Image *out) { return start_image(ph, start, out, SPB_G1); }
+
+int sp_phaser_start_model_before_projection(SpPhaser *ph, int start, Image *out) {
+  return start_image(ph, start, out, SPB_GP);
+}
+
+int sp_phaser_start_support(SpPhaser *ph, int start, Image *out) {
+  if (!out || sp_image_x(out) != ph->nx || sp_image_y(out) != ph->ny || sp_image_z(out) != ph->nz) return -1;
+  if (sync_to_device(ph)) return -8;
+  int *f = (int *)malloc(sizeof(int) * (size_t)ph->image_size);
+  if (spb_ctx_get_start_flags(state(ph)->ctx, start, f)) {
+    free(f);
+    return dev_error("download start support");
+  }
+  for (int i = 0; i < ph->image_size; i++) out->image->data[i] = sp_cinit((f[i] & SpPixelInsideSupport) ? 1 : 0, 0);
+  free(f);
+  return 0;
+}
+
+int sp_phaser_starts_efourier(SpPhaser *ph, real *out, real *FcFo) {
+  if (sync_to_device(ph)) return -8;
+  const int nb = sp_phaser_starts(ph);
+  double *s = (double *)malloc(sizeof(double) * 4 * (size_t)nb);
+  if (spb_ctx_batch_efourier_sums(state(ph)->ctx, s)) {
+    free(s);
+    return dev_error("efourier");
+  }
+  for (int b = 0; b < nb; b++) {
+    out[b] = (real)sqrt(s[4 * b] / s[4 * b + 1]);
+    if (FcFo) FcFo[b] = (real)(s[4 * b + 2] / s[4 * b + 3]);
+  }
+  free(s);
+  return 0;
+}
+
+int sp_phaser_starts_ereal(SpPhaser *ph, real *out) {
+  if (ensure_ctx(ph)) return -8;
+  const int nb = sp_phaser_starts(ph);
+  double *s = (double *)malloc(sizeof(double) * 4 * (size_t)nb);
+  if (spb_ctx_batch_ereal_sums(state(ph)->ctx, s)) {
+    free(s);
+    return dev_error("ereal");
+  }
+  for (int b = 0; b < nb; b++) out[b] = (real)sqrt(s[4 * b] / s[4 * b + 1]);
+  free(s);
+  return 0;
+}
+
+int sp_phaser_starts_support_fraction(SpPhaser *ph, real *out) {
+  if (sync_to_device(ph)) return -8;
+  const int nb = sp_phaser_starts(ph);
+  long long *c = (long long *)malloc(sizeof(long long) * (size_t)nb);
+  if (spb_ctx_batch_support_counts(state(ph)->ctx, c)) {
+    free(c);
+    return dev_error("support fraction");
+  }
+  for (int b = 0; b < nb; b++) out[b] = (real)c[b] / (real)ph->image_size;
+  free(c);
   return 0;
 }
 

@@ -1,13 +1,18 @@
 // C-ABI device layer of the phasing path (include/spimage/spb_device.h).
 //
-// A context owns the device buffers of one phasing problem:
-//   amp[N] f32, flags[N] u8 (bit0 inside support, bit1 measured),
-//   g[2][N] c64 ping-pong iterates (g1 = model, g0 = old model),
-//   X[N] c64 = row FFT of g1 (kept valid between iterations),
-//   Y[N] c64 scratch of the column passes, gp[N] c64 (last model before
-//   projection), T[N] c64 and absb[N] f32 scratch of the support update,
-//   Xf/Yf[N] c64 for the difference map's second transform pair.
-// All work is enqueued on one non-blocking stream per context.
+// A context holds nb independent starts ("batch") of one nx*ny*nz problem;
+// a single phaser is nb = 1.  Per-start buffers are stacked start-major
+// (start b at offset b*N):
+//   flags[nb*N] u8 (bit0 inside support, bit1 measured),
+//   g[2][nb*N] c64 ping-pong iterates (g1 = model, g0 = old model),
+//   X[nb*N] c64 = row FFT of g1 (kept valid between iterations),
+//   Y[nb*N] c64 projection-pass output, gp[nb*N] c64 (last model before
+//   projection), T[nb*N] c64 and absb[nb*N] f32 support-update scratch,
+//   Xf/Yf[nb*N] c64 for the difference map's second transform pair.
+// Shared by all starts (one pattern): amp[N], amp_line[N], meas_bits,
+// amp_min/amp_max/phased_amp[N].
+// Rows of all starts form one tall row pass; column passes treat the start
+// index as one more outer dimension.  All work is enqueued on one stream.
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -104,16 +109,17 @@ int make_axis(Axis &ax, int n) {
 }
 
 // Largest line the staging buffers hold: two n-point complex lines per row in
-// shared memory (row pass) or per column tile of two columns (column pass).
+// shared memory (row pass) or per column tile (column pass).
 const int kMaxAxis = 8192;
-
-}  // namespace
-
 // iterations per captured graph (even: the iterate buffers return to their roles)
 const int kGraphIters = 16;
 const int kMaxGraphs = 8;
 // iterations whose beta values one call can stage on the device
 const int kBetaCap = 1 << 16;
+// grid y-dimension limit of the column passes
+const int kMaxGridY = 65535;
+
+}  // namespace
 
 struct GraphEntry {
   bool used = false;
@@ -135,7 +141,9 @@ struct KernelProfile {
 
 struct spb_ctx {
   int nx = 0, ny = 0, nz = 0;
-  long long n = 0;
+  long long n = 0;     // pixels per start
+  int nb = 1;          // starts
+  long long ntot = 0;  // nb * n
   cudaStream_t st = nullptr;      // active stream
   cudaStream_t own_st = nullptr;  // the context's own stream
   KernelProfile prof;
@@ -162,9 +170,8 @@ struct spb_ctx {
   int beta_cap = 0;
   int *beta_base = nullptr;
   cudaEvent_t beta_ev = nullptr;
-  SelectState *sel = nullptr;
-  double *red = nullptr;
-  unsigned long long *cnt = nullptr;
+  SelectState *sel = nullptr;  // one per start
+  double *red = nullptr;       // reduce_scratch_doubles(nb)
   int x_valid = 0, xf_valid = 0;
   float xf_gamma1 = 0.0f;
 };
@@ -177,7 +184,8 @@ PassArgs base_args(const spb_ctx *c) {
   a.nx = c->nx;
   a.ny = c->ny;
   a.nz = c->nz;
-  a.n = c->n;
+  a.n = c->ntot;
+  a.n_start = c->n;
   a.amp = c->amp;
   a.amp_min = c->amin;
   a.amp_max = c->amax;
@@ -192,25 +200,26 @@ PassArgs base_args(const spb_ctx *c) {
   return a;
 }
 
-// Column-line geometry: axis 1 = y lines (per z slab), 2 = z lines, 0 = lines
-// of length 1 over every pixel (pointwise pass for 1-D problems).
+// Column-line geometry: axis 1 = y lines (one set per z slab of every start),
+// 2 = z lines (one set per start), 0 = lines of length 1 over every pixel
+// (pointwise pass for 1-D problems).
 void col_geometry(const spb_ctx *c, int axis, PassArgs &a, const LinePlan **pl) {
   if (axis == 1) {
     a.estride = c->nx;
     a.ostride = (long long)c->nx * c->ny;
     a.ncols = c->nx;
-    a.nouter = c->nz;
+    a.nouter = c->nb * c->nz;
     *pl = &c->ay.lp;
   } else if (axis == 2) {
     a.estride = (long long)c->nx * c->ny;
-    a.ostride = 0;
+    a.ostride = c->n;
     a.ncols = c->nx * c->ny;
-    a.nouter = 1;
+    a.nouter = c->nb;
     *pl = &c->az.lp;
   } else {
     a.estride = 1;
     a.ostride = 0;
-    a.ncols = (int)c->n;
+    a.ncols = (int)c->ntot;
     a.nouter = 1;
     *pl = nullptr;
   }
@@ -265,9 +274,14 @@ int col(spb_ctx *c, int axis, int mode, const float2 *src, float2 *dst, PassArgs
   a.src = src;
   a.dst = dst;
   LinePlan unit = unit_plan();
+  const int nouter = a.nouter;
   if (prof_begin(c)) return -1;
-  CK(launch_col(mode, pl ? *pl : unit, pl ? pl->n : 1, a, c->st));
-  c->launches++;
+  for (int o0 = 0; o0 < nouter; o0 += kMaxGridY) {
+    a.outer0 = o0;
+    a.nouter = nouter - o0 < kMaxGridY ? nouter - o0 : kMaxGridY;
+    CK(launch_col(mode, pl ? *pl : unit, pl ? pl->n : 1, a, c->st));
+    c->launches++;
+  }
   return prof_end(c, 10 + mode);
 }
 
@@ -309,7 +323,7 @@ int forward_rest(spb_ctx *c, const float2 *src, float2 *dst) {
   const int k = other_axes(c, axes);
   PassArgs a = base_args(c);
   if (k == 0) {
-    if (src != dst) CK(cudaMemcpyAsync(dst, src, sizeof(float2) * c->n, cudaMemcpyDeviceToDevice, c->st));
+    if (src != dst) CK(cudaMemcpyAsync(dst, src, sizeof(float2) * c->ntot, cudaMemcpyDeviceToDevice, c->st));
     return 0;
   }
   const float2 *s = src;
@@ -326,7 +340,7 @@ int backward_rest(spb_ctx *c, const float2 *src, float2 *dst) {
   const int k = other_axes(c, axes);
   PassArgs a = base_args(c);
   if (k == 0) {
-    if (src != dst) CK(cudaMemcpyAsync(dst, src, sizeof(float2) * c->n, cudaMemcpyDeviceToDevice, c->st));
+    if (src != dst) CK(cudaMemcpyAsync(dst, src, sizeof(float2) * c->ntot, cudaMemcpyDeviceToDevice, c->st));
     return 0;
   }
   const float2 *s = src;
@@ -359,24 +373,35 @@ int ensure_xf(spb_ctx *c, float gamma1) {
   return 0;
 }
 
-int check_dims(int nx, int ny, int nz) {
-  if (nx < 1 || ny < 1 || nz < 1) return fail("invalid dimensions %d x %d x %d", nx, ny, nz);
+int check_dims(int nx, int ny, int nz, int nb) {
+  if (nx < 1 || ny < 1 || nz < 1 || nb < 1) return fail("invalid dimensions %d x %d x %d x %d", nx, ny, nz, nb);
   if (nx > kMaxAxis || ny > kMaxAxis || nz > kMaxAxis)
     return fail("axis longer than %d is not supported (%d x %d x %d)", kMaxAxis, nx, ny, nz);
+  if ((long long)nx * ny * nz * nb >= (1LL << 31)) return fail("more than 2^31 pixels in one context");
+  return 0;
+}
+
+int check_start(const spb_ctx *c, int start) {
+  if (start < 0 || start >= c->nb) return fail("start %d out of range [0, %d)", start, c->nb);
   return 0;
 }
 
 }  // namespace
 
-extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
+extern "C" void spb_ctx_destroy(spb_ctx *c);
+
+extern "C" int spb_ctx_create_batch(spb_ctx **out, int nx, int ny, int nz, int nb) {
   *out = nullptr;
-  if (check_dims(nx, ny, nz)) return -1;
+  if (check_dims(nx, ny, nz, nb)) return -1;
   spb_ctx *c = new spb_ctx();
   c->nx = nx;
   c->ny = ny;
   c->nz = nz;
   c->n = (long long)nx * ny * nz;
-  const size_t nc = sizeof(float2) * (size_t)c->n, nf = sizeof(float) * (size_t)c->n;
+  c->nb = nb;
+  c->ntot = c->n * nb;
+  const size_t nc = sizeof(float2) * (size_t)c->ntot, nf = sizeof(float) * (size_t)c->ntot;
+  const size_t nf1 = sizeof(float) * (size_t)c->n;
   int rc = 0;
   auto alloc = [&](void **p, size_t bytes) {
     if (rc) return;
@@ -389,8 +414,8 @@ extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
     return fail("cudaStreamCreate: %s", cudaGetErrorString(e));
   }
   c->st = c->own_st;
-  alloc((void **)&c->amp, nf);
-  alloc((void **)&c->flags, (size_t)c->n);
+  alloc((void **)&c->amp, nf1);
+  alloc((void **)&c->flags, (size_t)c->ntot);
   alloc((void **)&c->g[0], nc);
   alloc((void **)&c->g[1], nc);
   alloc((void **)&c->X, nc);
@@ -398,9 +423,8 @@ extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
   alloc((void **)&c->gp, nc);
   alloc((void **)&c->T, nc);
   alloc((void **)&c->absb, nf);
-  alloc((void **)&c->sel, sizeof(SelectState));
-  alloc((void **)&c->red, sizeof(double) * (4 + 4 * 592));
-  alloc((void **)&c->cnt, sizeof(unsigned long long));
+  alloc((void **)&c->sel, sizeof(SelectState) * (size_t)nb);
+  alloc((void **)&c->red, sizeof(double) * (size_t)reduce_scratch_doubles(nb));
   alloc((void **)&c->beta_base, sizeof(int));
   alloc((void **)&c->beta_dev, sizeof(float) * kBetaCap);
   if (!rc && cudaMallocHost(&c->beta_pinned, sizeof(float) * kBetaCap) != cudaSuccess) rc = fail("cudaMallocHost");
@@ -411,8 +435,8 @@ extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
   if (!rc && make_axis(c->ay, ny)) rc = -1;
   if (!rc && make_axis(c->az, nz)) rc = -1;
   if (!rc) {
-    cudaMemsetAsync(c->amp, 0, nf, c->st);
-    cudaMemsetAsync(c->flags, 0, (size_t)c->n, c->st);
+    cudaMemsetAsync(c->amp, 0, nf1, c->st);
+    cudaMemsetAsync(c->flags, 0, (size_t)c->ntot, c->st);
     cudaMemsetAsync(c->g[0], 0, nc, c->st);
     cudaMemsetAsync(c->g[1], 0, nc, c->st);
     cudaMemsetAsync(c->gp, 0, nc, c->st);
@@ -427,20 +451,24 @@ extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
   return 0;
 }
 
+extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
+  return spb_ctx_create_batch(out, nx, ny, nz, 1);
+}
+
+extern "C" int spb_ctx_starts(spb_ctx *c) { return c->nb; }
+
 extern "C" void spb_ctx_destroy(spb_ctx *c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
-                  c->gp, c->T, c->absb, c->sel, c->red, c->cnt, c->ax.tw, c->ay.tw, c->az.tw,
-                  c->amp_line, c->meas_bits};
+                  c->gp, c->T, c->absb, c->sel, c->red, c->ax.tw, c->ay.tw, c->az.tw,
+                  c->amp_line, c->meas_bits, c->beta_dev, c->beta_base};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : c->prof.ev) cudaEventDestroy(e);
   for (auto &g : c->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
-  if (c->beta_dev) cudaFree(c->beta_dev);
   if (c->beta_pinned) cudaFreeHost(c->beta_pinned);
-  if (c->beta_base) cudaFree(c->beta_base);
   if (c->beta_ev) cudaEventDestroy(c->beta_ev);
   if (c->own_st) cudaStreamDestroy(c->own_st);
   delete c;
@@ -448,6 +476,51 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
 
 extern "C" int spb_ctx_synchronize(spb_ctx *c) {
   CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+static const char *kKernelNames[SPB_KERNEL_KINDS] = {
+    "row_fwd",        "row_fwd_dephase", "row_inv",     "row_inv_scale", "row_inv_abs",
+    "row_iter",       "row_dm_f1_fwd",   "row_dm_iter", "row_fwd_f32",   "row_fwd_square_f32",
+    "col_fwd",        "col_inv",         "col_project", "col_project_nofc", "col_blur",
+    "col_inv_square", "select_area",     "select_max",  "unused18",      "unused19"};
+
+extern "C" const char *spb_kernel_name(int kind) {
+  return (kind >= 0 && kind < SPB_KERNEL_KINDS) ? kKernelNames[kind] : "";
+}
+
+extern "C" int spb_ctx_profile(spb_ctx *c, int enable) {
+  KernelProfile &p = c->prof;
+  if (enable && p.ev.empty()) {
+    p.ev.resize(2 * kProfPairs);
+    p.kind.resize(kProfPairs);
+    for (auto &e : p.ev) CK(cudaEventCreate(&e));
+  }
+  if (!enable && prof_flush(c)) return -1;
+  p.on = enable != 0;
+  if (enable) {
+    for (int k = 0; k < SPB_KERNEL_KINDS; k++) {
+      p.launches[k] = 0;
+      p.ms[k] = 0;
+    }
+  }
+  return 0;
+}
+
+extern "C" int spb_ctx_profile_read(spb_ctx *c, int kind, long long *launches, double *total_ms) {
+  if (kind < 0 || kind >= SPB_KERNEL_KINDS) return fail("bad kernel kind %d", kind);
+  if (prof_flush(c)) return -1;
+  *launches = c->prof.launches[kind];
+  *total_ms = c->prof.ms[kind];
+  return 0;
+}
+
+extern "C" long long spb_ctx_launch_count(spb_ctx *c) { return c->launches; }
+
+extern "C" int spb_ctx_set_stream(spb_ctx *c, void *stream) {
+  if (prof_flush(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
+  c->st = stream ? (cudaStream_t)stream : c->own_st;
   return 0;
 }
 
@@ -473,7 +546,7 @@ __global__ void build_amp_line_kernel(const float *amp, float *amp_line, int len
     amp_line[k] = amp[i * estride + L];
   }
 }
-// bit i of line L = measured flag of pixel i*estride + L
+// bit i of line L = measured flag of pixel i*estride + L (of start 0)
 __global__ void build_meas_bits_kernel(const uint8_t *flags, uint32_t *bits, int len, int W, long long estride,
                                        long long nlines) {
   const long long total = nlines * W;
@@ -486,6 +559,15 @@ __global__ void build_meas_bits_kernel(const uint8_t *flags, uint32_t *bits, int
       if (i < len && (flags[i * estride + L] & FLAG_MEASURED)) word |= 1u << b;
     }
     bits[k] = word;
+  }
+}
+// every start's flags = start 0's (bits in `mask`), keeping the other bits
+__global__ void broadcast_flags_kernel(uint8_t *flags, long long n, int nb, uint8_t mask) {
+  const long long total = n * (nb - 1);
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const long long i = k % n;
+    uint8_t *f = flags + n + k;
+    *f = (uint8_t)((*f & ~mask) | (flags[i] & mask));
   }
 }
 }  // namespace spb
@@ -552,38 +634,69 @@ extern "C" int spb_ctx_set_phased_amplitudes(spb_ctx *c, const float *pa) {
   return upload(c, c->pamp, pa, nc);
 }
 
-extern "C" int spb_ctx_set_flags(spb_ctx *c, const int *flags) {
+static int put_flags(spb_ctx *c, int start, const int *flags) {
   std::vector<uint8_t> h((size_t)c->n);
   for (long long i = 0; i < c->n; i++) h[i] = (uint8_t)(flags[i] & 3);
-  if (upload(c, c->flags, h.data(), (size_t)c->n)) return -1;
+  return upload(c, c->flags + (size_t)start * c->n, h.data(), (size_t)c->n);
+}
+
+// every start gets these flags; measured bits feed the shared bitmap
+extern "C" int spb_ctx_set_flags(spb_ctx *c, const int *flags) {
+  if (put_flags(c, 0, flags)) return -1;
+  if (c->nb > 1) {
+    broadcast_flags_kernel<<<592, 256, 0, c->st>>>(c->flags, c->n, c->nb, 3);
+    CK(cudaGetLastError());
+  }
   if (build_meas_bits(c)) return -1;
   CK(cudaStreamSynchronize(c->st));
   c->xf_valid = 0;
   return 0;
 }
 
-extern "C" int spb_ctx_get_flags(spb_ctx *c, int *flags) {
+// one start's flags; its measured bits must equal start 0's (one pattern)
+extern "C" int spb_ctx_set_start_flags(spb_ctx *c, int start, const int *flags) {
+  if (check_start(c, start)) return -1;
+  if (put_flags(c, start, flags)) return -1;
+  if (start == 0 && build_meas_bits(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
+  c->xf_valid = 0;
+  return 0;
+}
+
+extern "C" int spb_ctx_get_start_flags(spb_ctx *c, int start, int *flags) {
+  if (check_start(c, start)) return -1;
   std::vector<uint8_t> h((size_t)c->n);
-  if (download(c, h.data(), c->flags, (size_t)c->n)) return -1;
+  if (download(c, h.data(), c->flags + (size_t)start * c->n, (size_t)c->n)) return -1;
   for (long long i = 0; i < c->n; i++) flags[i] = h[i];
   return 0;
 }
 
+extern "C" int spb_ctx_get_flags(spb_ctx *c, int *flags) { return spb_ctx_get_start_flags(c, 0, flags); }
+
 static int reset_iterates(spb_ctx *c) {
-  const size_t nc = sizeof(float2) * (size_t)c->n;
+  const size_t nc = sizeof(float2) * (size_t)c->ntot;
   CK(cudaMemsetAsync(c->g[c->cur ^ 1], 0, nc, c->st));
   CK(cudaMemsetAsync(c->gp, 0, nc, c->st));
   return 0;
 }
 
-extern "C" int spb_ctx_set_model(spb_ctx *c, const float *model, int reset_others) {
-  if (upload(c, c->g[c->cur], model, sizeof(float2) * (size_t)c->n)) return -1;
+extern "C" int spb_ctx_set_start_model(spb_ctx *c, int start, const float *model, int reset_others) {
+  if (check_start(c, start)) return -1;
+  if (upload(c, c->g[c->cur] + (size_t)start * c->n, model, sizeof(float2) * (size_t)c->n)) return -1;
   c->x_valid = c->xf_valid = 0;
   if (reset_others && reset_iterates(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
   return 0;
 }
 
-// g1 = backward FFT(T) * (1/N)
+// the same model for every start
+extern "C" int spb_ctx_set_model(spb_ctx *c, const float *model, int reset_others) {
+  for (int b = 0; b < c->nb; b++)
+    if (spb_ctx_set_start_model(c, b, model, reset_others && b == 0)) return -1;
+  return 0;
+}
+
+// g1 = backward FFT(T) * (1/N), every start
 static int inverse_scaled_into_model(spb_ctx *c) {
   if (backward_rest(c, c->T, c->T)) return -1;
   PassArgs a = base_args(c);
@@ -594,12 +707,75 @@ static int inverse_scaled_into_model(spb_ctx *c) {
   return 0;
 }
 
-extern "C" int spb_ctx_model_from_fourier(spb_ctx *c, const float *fourier, int reset_others) {
-  CK(cudaMemcpyAsync(c->T, fourier, sizeof(float2) * (size_t)c->n, cudaMemcpyHostToDevice, c->st));
+// fourier holds nb spectra (start-major), or one spectrum when `one` is set
+static int models_from_fourier(spb_ctx *c, const float *fourier, int one, int reset_others) {
+  const size_t ns = sizeof(float2) * (size_t)c->n;
+  for (int b = 0; b < c->nb; b++)
+    CK(cudaMemcpyAsync(c->T + (size_t)b * c->n, fourier + (one ? 0 : 2 * (size_t)b * c->n), ns,
+                       cudaMemcpyHostToDevice, c->st));
   if (inverse_scaled_into_model(c)) return -1;
   if (reset_others && reset_iterates(c)) return -1;
   CK(cudaStreamSynchronize(c->st));
   return 0;
+}
+
+extern "C" int spb_ctx_model_from_fourier(spb_ctx *c, const float *fourier, int reset_others) {
+  return models_from_fourier(c, fourier, 1, reset_others);
+}
+
+extern "C" int spb_ctx_models_from_fourier(spb_ctx *c, const float *fourier, int reset_others) {
+  return models_from_fourier(c, fourier, 0, reset_others);
+}
+
+namespace spb {
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror and Shaw, "Parallel
+// random numbers: as easy as 1, 2, 3", SC 2011): 10 rounds of two 32x32->64
+// multiplies, key bumped by the Weyl constants between rounds.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 ctr, uint2 key) {
+  for (int r = 0; r < 10; r++) {
+    const unsigned lo0 = 0xD2511F53u * ctr.x, hi0 = __umulhi(0xD2511F53u, ctr.x);
+    const unsigned lo1 = 0xCD9E8D57u * ctr.z, hi1 = __umulhi(0xCD9E8D57u, ctr.z);
+    ctr = make_uint4(hi1 ^ ctr.y ^ key.x, lo1, hi0 ^ ctr.w ^ key.y, lo0);
+    key.x += 0x9E3779B9u;
+    key.y += 0xBB67AE85u;
+  }
+  return ctr;
+}
+
+// T[b][i] = amp[i] * exp(2 pi i u), u uniform in [0,1) from (seed_b, i)
+__global__ void random_phase_spectra_kernel(float2 *T, const float *amp, const unsigned long long *seeds, long long n,
+                                            int nb) {
+  const long long total = n * nb;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(k / n);
+    const long long i = k % n;
+    const unsigned long long s = seeds[b];
+    const uint4 r = philox4x32_10(make_uint4((unsigned)i, (unsigned)(i >> 32), 0u, 0u),
+                                  make_uint2((unsigned)s, (unsigned)(s >> 32)));
+    const float u = (float)(r.x >> 8) * (1.0f / 16777216.0f);
+    float sn, cs;
+    sincospif(2.0f * u, &sn, &cs);
+    const float a = amp[i];
+    T[k] = make_float2(a * cs, a * sn);
+  }
+}
+}  // namespace spb
+
+// Random-phase starts drawn on the device (throughput runs; the host API's
+// SpModelRandomPhases path reproduces the reference's rand() sequence instead)
+extern "C" int spb_ctx_random_phase_models(spb_ctx *c, const unsigned long long *seeds, int reset_others) {
+  unsigned long long *ds = nullptr;
+  CK(cudaMalloc(&ds, sizeof(unsigned long long) * (size_t)c->nb));
+  int rc = upload(c, ds, seeds, sizeof(unsigned long long) * (size_t)c->nb);
+  if (!rc) {
+    random_phase_spectra_kernel<<<1184, 256, 0, c->st>>>(c->T, c->amp, ds, c->n, c->nb);
+    if (cudaGetLastError() != cudaSuccess) rc = fail("random phase kernel launch failed");
+  }
+  if (!rc) rc = inverse_scaled_into_model(c);
+  if (!rc && reset_others) rc = reset_iterates(c);
+  if (!rc && cudaStreamSynchronize(c->st) != cudaSuccess) rc = fail("random phase models failed");
+  cudaFree(ds);
+  return rc;
 }
 
 namespace spb {
@@ -615,15 +791,16 @@ extern "C" int spb_ctx_mask_out_unmeasured(spb_ctx *c) {
   a.dst = c->T;
   if (row(c, ROW_FWD, a)) return -1;
   if (forward_rest(c, c->T, c->T)) return -1;
-  zero_unmeasured_kernel<<<592, 256, 0, c->st>>>(c->T, c->flags, c->n);
+  zero_unmeasured_kernel<<<592, 256, 0, c->st>>>(c->T, c->flags, c->ntot);
   CK(cudaGetLastError());
   if (inverse_scaled_into_model(c)) return -1;
   CK(cudaStreamSynchronize(c->st));
   return 0;
 }
 
-// One iteration: g0 <- g1 (buffer roles swap), X -> Y (projection pass) ->
-// row pass writing g1 and the next X.  `a` carries the algorithm scalars.
+// One iteration of every start: g0 <- g1 (buffer roles swap), X -> Y
+// (projection pass) -> row pass writing g1 and the next X.  `a` carries the
+// algorithm scalars.
 static int one_iteration(spb_ctx *c, PassArgs a, float2 *gp_out) {
   c->cur ^= 1;
   a.g0 = c->g[c->cur ^ 1];
@@ -699,7 +876,10 @@ static GraphEntry *find_graph(spb_ctx *c, const spb_alg_desc *d) {
 static GraphEntry *new_graph_slot(spb_ctx *c, const spb_alg_desc *d) {
   GraphEntry *slot = nullptr;
   for (auto &g : c->graphs)
-    if (!g.used) { slot = &g; break; }
+    if (!g.used) {
+      slot = &g;
+      break;
+    }
   if (!slot) {
     slot = &c->graphs[c->graph_evict];
     c->graph_evict = (c->graph_evict + 1) % kMaxGraphs;
@@ -745,7 +925,7 @@ extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float 
   if (alg->objective == 0 && !c->amp) return fail("amplitudes not set");
   if (alg->objective == 1 && !c->pamp) return fail("phased amplitudes not set");
   if ((alg->constraints & C_MARGIN) && (!c->amin || !c->amax)) return fail("amplitude margins not set");
-  const size_t nc = sizeof(float2) * (size_t)c->n;
+  const size_t nc = sizeof(float2) * (size_t)c->ntot;
   if (A == ALG_DM) {
     if (!c->Xf) CK(cudaMalloc(&c->Xf, nc));
     if (!c->Yf) CK(cudaMalloc(&c->Yf, nc));
@@ -806,7 +986,7 @@ extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float 
   return 0;
 }
 
-// blur |g1| (or |img| when img != nullptr) into c->absb
+// blur |g1| of every start (or |img| when img != nullptr) into c->absb
 static int blur_abs(spb_ctx *c, const float2 *img, float radius) {
   PassArgs a = base_args(c);
   a.src = img ? img : c->g[c->cur];
@@ -824,99 +1004,70 @@ static int blur_abs(spb_ctx *c, const float2 *img, float radius) {
 // Area rule: threshold = k-th largest |blur| with k = (int)(N * area) (float
 // product, as the reference indexes its descending sort); k is clamped to
 // N-1 where the reference would read past the end.  Threshold rule: max|blur|
-// times value.  Then inside = |blur| > threshold.
-static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *absv, long long n, int type,
+// times value.  Then inside = |blur| > threshold.  nb starts of n pixels,
+// each with its own selection state.
+static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *absv, long long n, int nb, int type,
                               float value, uint8_t *flags) {
   if (type == SPB_SUPPORT_AREA) {
     long long k = (long long)(int)((float)n * value);
     if (k >= n) k = n - 1;
     if (k < 0) k = 0;
-    CK(launch_select_kth_desc(absv, n, k, sel, st));
-    CK(launch_mask_from_abs(absv, (const float *)sel, 0.0f, 0, flags, n, st));
+    CK(launch_select_kth_desc(absv, n, nb, k, sel, st));
+    CK(launch_mask_from_abs(absv, sel, 0.0f, 0, flags, n, nb, st));
   } else if (type == SPB_SUPPORT_THRESHOLD) {
-    CK(launch_max_abs(absv, n, sel, st));
-    CK(launch_mask_from_abs(absv, (const float *)sel, value, 1, flags, n, st));
+    CK(launch_max_abs(absv, n, nb, sel, st));
+    CK(launch_mask_from_abs(absv, sel, value, 1, flags, n, nb, st));
   } else {
     return fail("unknown support update type %d", type);
   }
   return 0;
 }
 
-static int select_and_mask(spb_ctx *c, const float *absv, long long n, int type, float value, uint8_t *flags) {
+static int select_and_mask(spb_ctx *c, const float *absv, long long n, int nb, int type, float value,
+                           uint8_t *flags) {
   if (prof_begin(c)) return -1;
-  if (select_and_mask_on(c->st, c->sel, absv, n, type, value, flags)) return -1;
+  if (select_and_mask_on(c->st, c->sel, absv, n, nb, type, value, flags)) return -1;
   c->launches += (type == SPB_SUPPORT_AREA) ? 10 : 4;
   return prof_end(c, type == SPB_SUPPORT_AREA ? 16 : 17);
 }
 
-static const char *kKernelNames[SPB_KERNEL_KINDS] = {
-    "row_fwd",        "row_fwd_dephase", "row_inv",     "row_inv_scale", "row_inv_abs",
-    "row_iter",       "row_dm_f1_fwd",   "row_dm_iter", "row_fwd_f32",   "row_fwd_square_f32",
-    "col_fwd",        "col_inv",         "col_project", "col_project_nofc", "col_blur",
-    "col_inv_square", "select_area",     "select_max",  "unused18",      "unused19"};
-
-extern "C" const char *spb_kernel_name(int kind) {
-  return (kind >= 0 && kind < SPB_KERNEL_KINDS) ? kKernelNames[kind] : "";
-}
-
-extern "C" int spb_ctx_profile(spb_ctx *c, int enable) {
-  KernelProfile &p = c->prof;
-  if (enable && p.ev.empty()) {
-    p.ev.resize(2 * kProfPairs);
-    p.kind.resize(kProfPairs);
-    for (auto &e : p.ev) CK(cudaEventCreate(&e));
-  }
-  if (!enable && prof_flush(c)) return -1;
-  p.on = enable != 0;
-  if (enable) {
-    for (int k = 0; k < SPB_KERNEL_KINDS; k++) {
-      p.launches[k] = 0;
-      p.ms[k] = 0;
-    }
-  }
-  return 0;
-}
-
-extern "C" int spb_ctx_profile_read(spb_ctx *c, int kind, long long *launches, double *total_ms) {
-  if (kind < 0 || kind >= SPB_KERNEL_KINDS) return fail("bad kernel kind %d", kind);
-  if (prof_flush(c)) return -1;
-  *launches = c->prof.launches[kind];
-  *total_ms = c->prof.ms[kind];
-  return 0;
-}
-
-extern "C" long long spb_ctx_launch_count(spb_ctx *c) { return c->launches; }
-
-extern "C" int spb_ctx_set_stream(spb_ctx *c, void *stream) {
-  if (prof_flush(c)) return -1;
-  CK(cudaStreamSynchronize(c->st));
-  c->st = stream ? (cudaStream_t)stream : c->own_st;
-  return 0;
-}
-
 extern "C" int spb_ctx_support_update(spb_ctx *c, int type, float radius, float value) {
   if (blur_abs(c, nullptr, radius)) return -1;
-  if (select_and_mask(c, c->absb, c->n, type, value, c->flags)) return -1;
+  if (select_and_mask(c, c->absb, c->n, c->nb, type, value, c->flags)) return -1;
   c->xf_valid = 0;
   return 0;
 }
 
+// Patterson support of the shared pattern, computed once on start 0's slot
+// and copied to every start.
 extern "C" int spb_ctx_support_patterson(spb_ctx *c, float value) {
+  const int nb = c->nb;
+  const long long ntot = c->ntot;
+  c->nb = 1;  // single-start geometry for the passes below
+  c->ntot = c->n;
+  int rc = 0;
   int axes[2];
   const int k = other_axes(c, axes);
   PassArgs a = base_args(c);
   a.f32src = c->amp;
   if (k == 0) {
-    if (col(c, 0, COL_INV_SQUARE_F32, nullptr, c->T, a)) return -1;
+    rc = col(c, 0, COL_INV_SQUARE_F32, nullptr, c->T, a);
   } else {
-    if (col(c, axes[k - 1], COL_INV_SQUARE_F32, nullptr, c->T, a)) return -1;
-    for (int i = k - 2; i >= 0; i--)
-      if (col(c, axes[i], COL_INV, c->T, c->T, a)) return -1;
+    rc = col(c, axes[k - 1], COL_INV_SQUARE_F32, nullptr, c->T, a);
+    for (int i = k - 2; i >= 0 && !rc; i--) rc = col(c, axes[i], COL_INV, c->T, c->T, a);
   }
   a.src = c->T;
   a.absout = c->absb;
-  if (row(c, ROW_INV_ABS, a)) return -1;
-  if (select_and_mask(c, c->absb, c->n, SPB_SUPPORT_THRESHOLD, value, c->flags)) return -1;
+  if (!rc) rc = row(c, ROW_INV_ABS, a);
+  if (!rc) rc = select_and_mask(c, c->absb, c->n, 1, SPB_SUPPORT_THRESHOLD, value, c->flags);
+  c->nb = nb;
+  c->ntot = ntot;
+  if (rc) return -1;
+  if (nb > 1) {
+    broadcast_flags_kernel<<<592, 256, 0, c->st>>>(c->flags, c->n, nb, FLAG_INSIDE);
+    CK(cudaGetLastError());
+    c->launches++;
+  }
   c->xf_valid = 0;
   CK(cudaStreamSynchronize(c->st));
   return 0;
@@ -927,7 +1078,8 @@ static int fmodel_into_T(spb_ctx *c) {
   return forward_rest(c, c->X, c->T);
 }
 
-extern "C" int spb_ctx_get_image(spb_ctx *c, int which, float *out) {
+extern "C" int spb_ctx_get_start_image(spb_ctx *c, int start, int which, float *out) {
+  if (check_start(c, start)) return -1;
   const size_t nc = sizeof(float2) * (size_t)c->n;
   const float2 *src = nullptr;
   switch (which) {
@@ -940,25 +1092,56 @@ extern "C" int spb_ctx_get_image(spb_ctx *c, int which, float *out) {
       break;
     default: return fail("unknown image %d", which);
   }
-  return download(c, out, src, nc);
+  return download(c, out, src + (size_t)start * c->n, nc);
+}
+
+extern "C" int spb_ctx_get_image(spb_ctx *c, int which, float *out) {
+  return spb_ctx_get_start_image(c, 0, which, out);
+}
+
+// sums[b*4 + k] for every start
+extern "C" int spb_ctx_batch_efourier_sums(spb_ctx *c, double *sums) {
+  if (fmodel_into_T(c)) return -1;
+  CK(launch_reduce_efourier(c->T, c->amp, c->flags, c->n, c->nb, c->red, c->st));
+  c->launches += 2;
+  return download(c, sums, c->red, sizeof(double) * 4 * (size_t)c->nb);
+}
+
+extern "C" int spb_ctx_batch_ereal_sums(spb_ctx *c, double *sums) {
+  CK(launch_reduce_ereal(c->gp, c->flags, c->n, c->nb, c->red, c->st));
+  c->launches += 2;
+  return download(c, sums, c->red, sizeof(double) * 4 * (size_t)c->nb);
+}
+
+// counts[b] = pixels inside start b's support
+extern "C" int spb_ctx_batch_support_counts(spb_ctx *c, long long *counts) {
+  CK(launch_count_inside(c->flags, c->n, c->nb, c->red, c->st));
+  c->launches += 2;
+  std::vector<double> h((size_t)c->nb * 4);
+  if (download(c, h.data(), c->red, sizeof(double) * h.size())) return -1;
+  for (int b = 0; b < c->nb; b++) counts[b] = (long long)h[(size_t)b * 4];
+  return 0;
 }
 
 extern "C" int spb_ctx_efourier_sums(spb_ctx *c, double sums[4]) {
-  if (fmodel_into_T(c)) return -1;
-  CK(launch_reduce_efourier(c->T, c->amp, c->flags, c->n, c->red, c->st));
-  return download(c, sums, c->red, sizeof(double) * 4);
+  std::vector<double> h((size_t)c->nb * 4);
+  if (spb_ctx_batch_efourier_sums(c, h.data())) return -1;
+  for (int k = 0; k < 4; k++) sums[k] = h[k];
+  return 0;
 }
 
 extern "C" int spb_ctx_ereal_sums(spb_ctx *c, double sums[2]) {
-  CK(launch_reduce_ereal(c->gp, c->flags, c->n, c->red, c->st));
-  return download(c, sums, c->red, sizeof(double) * 2);
+  std::vector<double> h((size_t)c->nb * 4);
+  if (spb_ctx_batch_ereal_sums(c, h.data())) return -1;
+  sums[0] = h[0];
+  sums[1] = h[1];
+  return 0;
 }
 
 extern "C" int spb_ctx_support_count(spb_ctx *c, long long *count) {
-  CK(launch_count_inside(c->flags, c->n, c->cnt, c->st));
-  unsigned long long v = 0;
-  if (download(c, &v, c->cnt, sizeof(v))) return -1;
-  *count = (long long)v;
+  std::vector<long long> h((size_t)c->nb);
+  if (spb_ctx_batch_support_counts(c, h.data())) return -1;
+  *count = h[0];
   return 0;
 }
 
@@ -1023,7 +1206,7 @@ static int support_from_blur_impl(long long n, const float *blur, int type, floa
   CK(cudaMemcpyAsync(dflags, h.data(), (size_t)n, cudaMemcpyHostToDevice, st));
   abs_kernel<<<592, 256, 0, st>>>(dblur, dabs, n);
   CK(cudaGetLastError());
-  if (select_and_mask_on(st, sel, dabs, n, type, value, dflags)) return -1;
+  if (select_and_mask_on(st, sel, dabs, n, 1, type, value, dflags)) return -1;
   CK(cudaMemcpyAsync(h.data(), dflags, (size_t)n, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   for (long long i = 0; i < n; i++) flags[i] = h[i];

@@ -72,6 +72,16 @@ struct Stages {
       if constexpr (LAST) {
 #pragma unroll
         for (int m = 0; m < R; m++) v[j + m * J] = a[m];
+      } else if constexpr (NS % 16 == 0) {
+        // m*NS leaves the low 4 bits of base alone: pad(base + m*NS) = pad(base) + m*(NS + NS/16)
+        float2 *p = line + pad((b / NS) * NS * R + k);
+#pragma unroll
+        for (int m = 0; m < R; m++) p[m * (NS + NS / 16)] = a[m];
+      } else if constexpr (NS == 1) {
+        // R divides 16 and m < R: pad(b*R + m) = pad(b*R) + m
+        float2 *p = line + pad(b * R);
+#pragma unroll
+        for (int m = 0; m < R; m++) p[m] = a[m];
       } else {
         const int base = (b / NS) * NS * R + k;
 #pragma unroll
@@ -80,8 +90,14 @@ struct Stages {
     }
     if constexpr (!LAST) {
       __syncthreads();
+      if constexpr (T % 16 == 0) {
+        const float2 *p = line + pad(t);
 #pragma unroll
-      for (int q = 0; q < 16; q++) v[q] = line[pad(t + T * q)];
+        for (int q = 0; q < 16; q++) v[q] = p[q * (T + T / 16)];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; q++) v[q] = line[pad(t + T * q)];
+      }
       __syncthreads();
       Stages<N, S + 1, NS * R, INV>::run(v, line, t, stw + (R - 1) * NS);
     }
@@ -117,18 +133,29 @@ __device__ __forceinline__ float2 project_with(float2 G, float amp, bool measure
                                                bool fourier_constraints) {
   if (fourier_constraints && (a.constraints & C_CENTROSYM)) G.y = 0.0f;
   if (!measured) return G;
-  if (a.objective != 0) return a.phased_amp[idx];
+  if (a.objective != 0) return a.phased_amp[idx % a.n_start];
   float m = 1.0f;
   if (!(a.constraints & C_MARGIN)) {
     m = __fdiv_rn(amp, cabs_ref(G));
   } else {
     const float av = cabs_ref(G);
-    const float lo = a.amp_min[idx], hi = a.amp_max[idx];
+    const float lo = a.amp_min[idx % a.n_start], hi = a.amp_max[idx % a.n_start];
     if (av < lo) m = __fdiv_rn(lo, av);
     else if (av > hi) m = __fdiv_rn(hi, av);
   }
   if (isfinite(m)) return make_float2(fmul(G.x, m), fmul(G.y, m));
   return make_float2(amp, 0.0f);
+}
+
+// words per line of the measured-bit bitmap (a multiple of 4 words)
+__host__ __device__ constexpr int proj_words(int n) { return ((n + 127) / 128) * 4; }
+template <int N, int C>
+__host__ __device__ constexpr int amp_stride() {
+  return N + (C == 1 ? 0 : (C <= 8 ? 32 / C : 4));
+}
+template <int N, int C>
+__host__ __device__ constexpr int bits_stride() {
+  return C == 1 ? proj_words(N) : proj_words(N) + ((((C <= 8 ? 32 / C : 4) - proj_words(N) % 32) + 32) % 32);
 }
 
 // ------------------------------------------------------------ row kernels
@@ -241,18 +268,28 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
   const bool valid = col < a.ncols;
   float2 *tw_s = sm;
   float2 *line = sm + N + c * S;
+  // staged operand lines: strides skewed so the C lines of a warp fall in
+  // different banks (multiples of 4 words keep the 16-byte copies aligned)
+  constexpr int W = proj_words(N);
+  constexpr int SA = amp_stride<N, C>();
+  constexpr int SW = bits_stride<N, C>();
   float *amp_s = reinterpret_cast<float *>(sm + N + C * S);
-  uint32_t *meas_s = reinterpret_cast<uint32_t *>(amp_s + C * N);
-  const int W = a.meas_words;
+  uint32_t *meas_s = reinterpret_cast<uint32_t *>(amp_s + C * SA);
   stage_twiddles<N>(tw_s, stw);
   if constexpr (PREFETCH) {
     const int vl = min(C, a.ncols - col0);
     const float *asrc = a.amp_line + (size_t)col0 * N;
-    for (int k = threadIdx.x; k < vl * N / 4; k += blockDim.x) cp_async16(amp_s + 4 * k, asrc + 4 * k);
+    for (int k = threadIdx.x; k < vl * (N / 4); k += blockDim.x) {
+      const int l = k / (N / 4), j = k % (N / 4);
+      cp_async16(amp_s + l * SA + 4 * j, asrc + (size_t)l * N + 4 * j);
+    }
     const uint32_t *msrc = a.meas_bits + (size_t)col0 * W;
-    for (int k = threadIdx.x; k < vl * W / 4; k += blockDim.x) cp_async16(meas_s + 4 * k, msrc + 4 * k);
+    for (int k = threadIdx.x; k < vl * (W / 4); k += blockDim.x) {
+      const int l = k / (W / 4), j = k % (W / 4);
+      cp_async16(meas_s + l * SW + 4 * j, msrc + (size_t)l * W + 4 * j);
+    }
   }
-  const size_t lbase = (size_t)blockIdx.y * a.ostride + col + (size_t)t * a.estride;
+  const size_t lbase = (size_t)(a.outer0 + blockIdx.y) * a.ostride + col + (size_t)t * a.estride;
   const size_t qstride = (size_t)T * a.estride;
   float2 v[16];
 #pragma unroll
@@ -283,8 +320,8 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
         const size_t idx = lbase + q * qstride;
         if constexpr (PREFETCH) {
           const int i = t + T * q;
-          const float amp = amp_s[c * N + i];
-          const bool meas = (meas_s[c * W + (i >> 5)] >> (i & 31)) & 1u;
+          const float amp = amp_s[c * SA + i];
+          const bool meas = (meas_s[c * SW + (i >> 5)] >> (i & 31)) & 1u;
           v[q] = project_with(v[q], amp, meas, idx, a, MODE == COL_PROJECT);
         } else if constexpr (MODE == COL_PROJECT) {
           v[q] = project(v[q], idx, a, true);
@@ -337,7 +374,10 @@ static cudaError_t col_fast_launch_p(const LinePlan &pl, const PassArgs &a, cuda
   constexpr int C = col_width<N>();
   constexpr int T = N / 16;
   size_t smem = (size_t)(N + C * (N + N / 16 + (C > 1 ? 16 / C : 0))) * sizeof(float2);
-  if (PREFETCH) smem += (size_t)C * N * sizeof(float) + (size_t)C * a.meas_words * sizeof(uint32_t);
+  if (PREFETCH) {
+    if (a.meas_words != proj_words(N)) return cudaErrorInvalidValue;
+    smem += (size_t)C * amp_stride<N, C>() * sizeof(float) + (size_t)C * bits_stride<N, C>() * sizeof(uint32_t);
+  }
   auto k = col_fast_kernel<N, MODE, C, PREFETCH>;
   static bool done = false;
   static size_t done_smem = 0;
@@ -353,7 +393,9 @@ static cudaError_t col_fast_launch_p(const LinePlan &pl, const PassArgs &a, cuda
 template <int N, int MODE>
 static cudaError_t col_fast_launch(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
   constexpr bool PROJ = (MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC);
-  if (PROJ && a.amp_line && a.meas_bits && (a.meas_words % 4) == 0 && a.nouter == 1)
+  // projection passes run along the last axis; every start (outer index)
+  // shares the line-major amplitude and measured-bit lines of its column
+  if (PROJ && a.amp_line && a.meas_bits && (a.meas_words % 4) == 0)
     return col_fast_launch_p<N, MODE, PROJ>(pl, a, st);
   return col_fast_launch_p<N, MODE, false>(pl, a, st);
 }

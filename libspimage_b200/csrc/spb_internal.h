@@ -48,6 +48,7 @@ struct PassArgs {
   // line addressing for column passes: addr = o*ostride + c + i*estride
   long long ostride, estride;
   int ncols, nouter;
+  long long outer0;  // first outer line of this launch (grids are split at 65535)
   // buffers
   const float2 *src;
   const float2 *src2;  // second input line (DM: Yf)
@@ -75,6 +76,9 @@ struct PassArgs {
   const int *beta_base;
   int beta_idx;
   float gamma1, gamma2, one_p_g2, size_f;
+  // pixels per start: the amplitude-side arrays (amp, amp_min, amp_max,
+  // phased_amp) hold one start and are indexed modulo n_start
+  long long n_start;
   // blur
   double blur_c0;   // -2*pow(pi,2) (host glibc)
   double blur_r2;   // pow(radius,2)
@@ -100,17 +104,19 @@ cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cud
 // general kernels otherwise
 cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArgs &a, cudaStream_t st);
-cudaError_t launch_mask_from_abs(const float *absv, const float *thr_dev, float rel, int use_rel, uint8_t *flags,
-                                 long long n, cudaStream_t st);
-cudaError_t launch_select_kth_desc(const float *absv, long long n, long long k, SelectState *state, cudaStream_t st);
-cudaError_t launch_max_abs(const float *absv, long long n, SelectState *state, cudaStream_t st);
-cudaError_t launch_reduce_efourier(const float2 *F, const float *amp, const uint8_t *flags, long long n,
-                                   double *out4, cudaStream_t st);
-cudaError_t launch_reduce_ereal(const float2 *gp, const uint8_t *flags, long long n, double *out2,
+// support selection and reductions; nb starts of n pixels each, start b at offset b*n
+cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long long k, SelectState *state,
+                                   cudaStream_t st);
+cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st);
+cudaError_t launch_mask_from_abs(const float *absv, const SelectState *state, float rel, int use_rel, uint8_t *flags,
+                                 long long n, int nb, cudaStream_t st);
+// out[b*4 + k]; scratch of reduce_scratch_doubles(nb) doubles starting at out
+int reduce_scratch_doubles(int nb);
+cudaError_t launch_reduce_efourier(const float2 *F, const float *amp, const uint8_t *flags, long long n, int nb,
+                                   double *out, cudaStream_t st);
+cudaError_t launch_reduce_ereal(const float2 *gp, const uint8_t *flags, long long n, int nb, double *out,
                                 cudaStream_t st);
-cudaError_t launch_count_inside(const uint8_t *flags, long long n, unsigned long long *out, cudaStream_t st);
-cudaError_t launch_flags_from_int(const int *src, uint8_t *dst, long long n, cudaStream_t st);
-cudaError_t launch_flags_to_int(const uint8_t *src, int *dst, long long n, cudaStream_t st);
+cudaError_t launch_count_inside(const uint8_t *flags, long long n, int nb, double *out, cudaStream_t st);
 cudaError_t launch_scale_cmul(float2 *a, long long n, float v, cudaStream_t st);
 
 }  // namespace spb

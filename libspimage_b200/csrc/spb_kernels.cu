@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
   extern __shared__ float2 smem[];
   const int n = pl.n;
   const int cc = threadIdx.x % ct, t = threadIdx.x / ct;
-  const long long o = blockIdx.y;
+  const long long o = a.outer0 + blockIdx.y;
   const int c = blockIdx.x * ct + cc;
   const bool valid = c < a.ncols;
   float2 *A = smem + cc;
@@ -267,18 +267,23 @@ cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArg
 }
 
 // ------------------------------------------------- support selection kernels
-// Exact k-th largest value by most-significant-digit radix select over the
-// float bit patterns (non-negative floats order like their bits): four passes
-// of 8 bits, each a histogram of the keys that match the digits fixed so far.
-// Histograms are kept per warp in shared memory and lanes holding the same
-// digit are combined with a match before the atomic, because the leading
-// digits of |blur| concentrate in a few bins.
+// Exact k-th largest value per start by most-significant-digit radix select
+// over the float bit patterns (non-negative floats order like their bits):
+// four passes of 8 bits, each a histogram of the keys that match the digits
+// fixed so far.  Histograms are kept per warp in shared memory and lanes
+// holding the same digit are combined with a match before the atomic,
+// because the leading digits of |blur| concentrate in a few bins.  Start b
+// owns v[b*n .. (b+1)*n) and state s[b]; the grid's y dimension runs over
+// starts.
 #define SEL_BITS 8
 #define SEL_BINS 256
 __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restrict__ v, long long n, SelectState *s,
                                                           int shift) {
   __shared__ unsigned int h[8][SEL_BINS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.y;
+  v += (long long)b * n;
+  s += b;
   for (int i = threadIdx.x; i < 8 * SEL_BINS; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
   const unsigned int prefix = s->prefix, pmask = s->prefix_mask;
@@ -303,17 +308,18 @@ __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restric
   }
 }
 
-// one warp: find the digit holding the rank-th largest key, narrow the prefix
-__global__ void select_pick_kernel(SelectState *s, int shift, int last) {
+// one warp per start: find the digit holding the rank-th largest key, narrow the prefix
+__global__ void select_pick_kernel(SelectState *states, int shift, int last) {
+  SelectState *s = states + blockIdx.x;
   const int lane = threadIdx.x;
-  // lane l owns digits [8l, 8l+8); counts of keys with a larger digit come from a suffix scan
+  // lane l owns digits [8l, 8l+8); counts of keys with a larger digit come from the higher lanes
   unsigned long long own = 0;
   unsigned int c[8];
   for (int j = 0; j < 8; j++) {
     c[j] = s->hist[lane * 8 + j];
     own += c[j];
   }
-  unsigned long long above = 0;  // keys whose digit is owned by a higher lane
+  unsigned long long above = 0;
   for (int l = 31; l > 0; l--) {
     const unsigned long long x = __shfl_sync(0xffffffffu, own, l);
     if (l > lane) above += x;
@@ -340,7 +346,8 @@ __global__ void select_pick_kernel(SelectState *s, int shift, int last) {
   for (int j = 0; j < 8; j++) s->hist[lane * 8 + j] = 0;
 }
 
-__global__ void select_init_kernel(SelectState *s, unsigned long long rank) {
+__global__ void select_init_kernel(SelectState *states, unsigned long long rank) {
+  SelectState *s = states + blockIdx.x;
   for (int d = threadIdx.x; d < 2048; d += blockDim.x) s->hist[d] = 0;
   if (threadIdx.x == 0) {
     s->prefix = 0;
@@ -350,20 +357,29 @@ __global__ void select_init_kernel(SelectState *s, unsigned long long rank) {
   }
 }
 
-cudaError_t launch_select_kth_desc(const float *absv, long long n, long long k, SelectState *state,
+static unsigned blocks_per_start(long long n, int nb) {
+  long long b = (n + 255) / 256;
+  long long cap = 148 * 4 / nb;
+  if (cap < 2) cap = 2;
+  if (b > cap) b = cap;
+  return (unsigned)(b > 0 ? b : 1);
+}
+
+cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long long k, SelectState *state,
                                    cudaStream_t st) {
-  select_init_kernel<<<1, 256, 0, st>>>(state, (unsigned long long)k);
-  long long blocks = (n + 255) / 256;
-  if (blocks > 148 * 4) blocks = 148 * 4;
+  select_init_kernel<<<nb, 256, 0, st>>>(state, (unsigned long long)k);
+  const dim3 grid(blocks_per_start(n, nb), nb);
   for (int p = 0; p < 4; p++) {
     const int shift = 24 - SEL_BITS * p;
-    select_hist_kernel<<<(unsigned)blocks, 256, 0, st>>>(absv, n, state, shift);
-    select_pick_kernel<<<1, 32, 0, st>>>(state, shift, p == 3);
+    select_hist_kernel<<<grid, 256, 0, st>>>(absv, n, state, shift);
+    select_pick_kernel<<<nb, 32, 0, st>>>(state, shift, p == 3);
   }
   return cudaGetLastError();
 }
 
-__global__ void max_abs_kernel(const float *__restrict__ v, long long n, SelectState *s) {
+__global__ void max_abs_kernel(const float *__restrict__ v, long long n, SelectState *states) {
+  SelectState *s = states + blockIdx.y;
+  v += (long long)blockIdx.y * n;
   unsigned int m = 0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const float x = v[i];
@@ -373,48 +389,65 @@ __global__ void max_abs_kernel(const float *__restrict__ v, long long n, SelectS
   if ((threadIdx.x & 31) == 0) atomicMax(&s->maxbits, m);
 }
 
-__global__ void max_finish_kernel(SelectState *s) { s->result = __uint_as_float(s->maxbits); }
+__global__ void max_finish_kernel(SelectState *states) {
+  SelectState *s = states + blockIdx.x;
+  s->result = __uint_as_float(s->maxbits);
+}
 
-cudaError_t launch_max_abs(const float *absv, long long n, SelectState *state, cudaStream_t st) {
-  select_init_kernel<<<1, 256, 0, st>>>(state, 0);
-  long long blocks = (n + 255) / 256;
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  max_abs_kernel<<<(unsigned)blocks, 256, 0, st>>>(absv, n, state);
-  max_finish_kernel<<<1, 1, 0, st>>>(state);
+cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st) {
+  select_init_kernel<<<nb, 256, 0, st>>>(state, 0);
+  max_abs_kernel<<<dim3(blocks_per_start(n, nb), nb), 256, 0, st>>>(absv, n, state);
+  max_finish_kernel<<<nb, 1, 0, st>>>(state);
   return cudaGetLastError();
 }
 
 // support_from_absolute_threshold (src/support_update.c:392-400): strict '>'
-__global__ void mask_kernel(const float *__restrict__ v, const SelectState *s, float rel, int use_rel,
+__global__ void mask_kernel(const float *__restrict__ v, const SelectState *states, float rel, int use_rel,
                             uint8_t *flags, long long n) {
+  const int b = blockIdx.y;
+  const SelectState *s = states + b;
   const float t = use_rel ? __fmul_rn(s->result, rel) : s->result;
+  v += (long long)b * n;
+  flags += (long long)b * n;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const uint8_t f = flags[i];
     flags[i] = (v[i] > t) ? (uint8_t)(f | FLAG_INSIDE) : (uint8_t)(f & ~FLAG_INSIDE);
   }
 }
 
-cudaError_t launch_mask_from_abs(const float *absv, const float *thr_dev, float rel, int use_rel, uint8_t *flags,
-                                 long long n, cudaStream_t st) {
-  (void)thr_dev;
-  long long blocks = (n + 255) / 256;
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  mask_kernel<<<(unsigned)blocks, 256, 0, st>>>(absv, reinterpret_cast<const SelectState *>(thr_dev), rel, use_rel,
-                                                flags, n);
+cudaError_t launch_mask_from_abs(const float *absv, const SelectState *state, float rel, int use_rel, uint8_t *flags,
+                                 long long n, int nb, cudaStream_t st) {
+  mask_kernel<<<dim3(blocks_per_start(n, nb), nb), 256, 0, st>>>(absv, state, rel, use_rel, flags, n);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- reductions
-#define RED_BLOCKS 592
+// Per start b: partial sums of blocks_per_start blocks into part[b][blk][4],
+// then one block per start adds them in a fixed order (deterministic).
+static __device__ void block_sum4(double s[4], double *out) {
+  __shared__ double sh[4][256];
+  for (int k = 0; k < 4; k++) sh[k][threadIdx.x] = s[k];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) out[k] = sh[k][0];
+}
 
 // efourier terms (src/phasing.c:852-891): nom, den, FcFo numerator, denominator
 __global__ void efourier_partial_kernel(const float2 *__restrict__ F, const float *__restrict__ amp,
                                         const uint8_t *__restrict__ flags, long long n, double *part) {
+  const int b = blockIdx.y;
+  F += (long long)b * n;
+  flags += (long long)b * n;
   double s[4] = {0, 0, 0, 0};
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const float fa = cabs_ref(F[i]);
     if (flags[i] & FLAG_MEASURED) {
-      const float aa = fabsf(amp[i]);
+      const float aa = cabs_ref(make_float2(amp[i], 0.0f));
       const double d = (double)__fsub_rn(fa, aa);
       s[0] += d * d;
       s[1] += (double)aa * (double)aa;
@@ -424,98 +457,65 @@ __global__ void efourier_partial_kernel(const float2 *__restrict__ F, const floa
       s[1] += (double)fa * (double)fa;
     }
   }
-  __shared__ double sh[4][256];
-  for (int k = 0; k < 4; k++) sh[k][threadIdx.x] = s[k];
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w)
-      for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 4; k++) part[blockIdx.x * 4 + k] = sh[k][0];
+  block_sum4(s, part + ((size_t)b * gridDim.x + blockIdx.x) * 4);
 }
 
 __global__ void ereal_partial_kernel(const float2 *__restrict__ gp, const uint8_t *__restrict__ flags, long long n,
                                      double *part) {
+  const int b = blockIdx.y;
+  gp += (long long)b * n;
+  flags += (long long)b * n;
   double s[4] = {0, 0, 0, 0};
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const double a = (double)cabs_ref(gp[i]);
     if (!(flags[i] & FLAG_INSIDE)) s[0] += a * a;
     s[1] += a * a;
   }
-  __shared__ double sh[4][256];
-  for (int k = 0; k < 4; k++) sh[k][threadIdx.x] = s[k];
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w)
-      for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 4; k++) part[blockIdx.x * 4 + k] = sh[k][0];
+  block_sum4(s, part + ((size_t)b * gridDim.x + blockIdx.x) * 4);
 }
 
-__global__ void finish4_kernel(const double *part, int nparts, double *out4) {
-  __shared__ double sh[4][256];
+__global__ void count_inside_partial_kernel(const uint8_t *__restrict__ flags, long long n, double *part) {
+  const int b = blockIdx.y;
+  flags += (long long)b * n;
+  double s[4] = {0, 0, 0, 0};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s[0] += (flags[i] & FLAG_INSIDE) ? 1.0 : 0.0;
+  block_sum4(s, part + ((size_t)b * gridDim.x + blockIdx.x) * 4);
+}
+
+__global__ void finish4_kernel(const double *part, int nparts, double *out) {
+  const int b = blockIdx.x;
   double s[4] = {0, 0, 0, 0};
   for (int i = threadIdx.x; i < nparts; i += blockDim.x)
-    for (int k = 0; k < 4; k++) s[k] += part[i * 4 + k];
-  for (int k = 0; k < 4; k++) sh[k][threadIdx.x] = s[k];
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w)
-      for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 4; k++) out4[k] = sh[k][0];
+    for (int k = 0; k < 4; k++) s[k] += part[((size_t)b * nparts + i) * 4 + k];
+  block_sum4(s, out + (size_t)b * 4);
 }
 
-cudaError_t launch_reduce_efourier(const float2 *F, const float *amp, const uint8_t *flags, long long n,
-                                   double *out4, cudaStream_t st) {
-  double *part = out4 + 4;
-  efourier_partial_kernel<<<RED_BLOCKS, 256, 0, st>>>(F, amp, flags, n, part);
-  finish4_kernel<<<1, 256, 0, st>>>(part, RED_BLOCKS, out4);
+int reduce_scratch_doubles(int nb) { return nb * 4 + nb * 4 * (int)blocks_per_start(1LL << 40, nb); }
+
+cudaError_t launch_reduce_efourier(const float2 *F, const float *amp, const uint8_t *flags, long long n, int nb,
+                                   double *out, cudaStream_t st) {
+  const unsigned bl = blocks_per_start(1LL << 40, nb);
+  double *part = out + (size_t)nb * 4;
+  efourier_partial_kernel<<<dim3(bl, nb), 256, 0, st>>>(F, amp, flags, n, part);
+  finish4_kernel<<<nb, 256, 0, st>>>(part, bl, out);
   return cudaGetLastError();
 }
 
-cudaError_t launch_reduce_ereal(const float2 *gp, const uint8_t *flags, long long n, double *out4,
+cudaError_t launch_reduce_ereal(const float2 *gp, const uint8_t *flags, long long n, int nb, double *out,
                                 cudaStream_t st) {
-  double *part = out4 + 4;
-  ereal_partial_kernel<<<RED_BLOCKS, 256, 0, st>>>(gp, flags, n, part);
-  finish4_kernel<<<1, 256, 0, st>>>(part, RED_BLOCKS, out4);
+  const unsigned bl = blocks_per_start(1LL << 40, nb);
+  double *part = out + (size_t)nb * 4;
+  ereal_partial_kernel<<<dim3(bl, nb), 256, 0, st>>>(gp, flags, n, part);
+  finish4_kernel<<<nb, 256, 0, st>>>(part, bl, out);
   return cudaGetLastError();
 }
 
-__global__ void count_inside_kernel(const uint8_t *flags, long long n, unsigned long long *out) {
-  unsigned long long c = 0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    c += (flags[i] & FLAG_INSIDE) ? 1 : 0;
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(out, c);
-}
-
-cudaError_t launch_count_inside(const uint8_t *flags, long long n, unsigned long long *out, cudaStream_t st) {
-  cudaMemsetAsync(out, 0, sizeof(unsigned long long), st);
-  count_inside_kernel<<<RED_BLOCKS, 256, 0, st>>>(flags, n, out);
-  return cudaGetLastError();
-}
-
-__global__ void flags_from_int_kernel(const int *src, uint8_t *dst, long long n) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    dst[i] = (uint8_t)(src[i] & 3);
-}
-__global__ void flags_to_int_kernel(const uint8_t *src, int *dst, long long n) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    dst[i] = (int)src[i];
-}
-cudaError_t launch_flags_from_int(const int *src, uint8_t *dst, long long n, cudaStream_t st) {
-  flags_from_int_kernel<<<RED_BLOCKS, 256, 0, st>>>(src, dst, n);
-  return cudaGetLastError();
-}
-cudaError_t launch_flags_to_int(const uint8_t *src, int *dst, long long n, cudaStream_t st) {
-  flags_to_int_kernel<<<RED_BLOCKS, 256, 0, st>>>(src, dst, n);
+cudaError_t launch_count_inside(const uint8_t *flags, long long n, int nb, double *out, cudaStream_t st) {
+  const unsigned bl = blocks_per_start(1LL << 40, nb);
+  double *part = out + (size_t)nb * 4;
+  count_inside_partial_kernel<<<dim3(bl, nb), 256, 0, st>>>(flags, n, part);
+  finish4_kernel<<<nb, 256, 0, st>>>(part, bl, out);
   return cudaGetLastError();
 }
 
@@ -524,7 +524,7 @@ __global__ void scale_cmul_kernel(float2 *a, long long n, float v) {
     a[i] = scale_cmul_dev(a[i], v);
 }
 cudaError_t launch_scale_cmul(float2 *a, long long n, float v, cudaStream_t st) {
-  scale_cmul_kernel<<<RED_BLOCKS, 256, 0, st>>>(a, n, v);
+  scale_cmul_kernel<<<592, 256, 0, st>>>(a, n, v);
   return cudaGetLastError();
 }
 

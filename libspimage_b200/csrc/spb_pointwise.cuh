@@ -34,16 +34,17 @@ __device__ __forceinline__ float2 apply_constraints(float2 g, uint8_t f, int c) 
 // Fourier-space projection at pixel idx (src/phasing.c:1061-1109)
 __device__ __forceinline__ float2 project(float2 G, long long idx, const PassArgs &a, bool fourier_constraints) {
   const uint8_t f = a.flags[idx];
+  const long long ai = idx % a.n_start;  // amplitude-side arrays hold one start
   if (fourier_constraints && (a.constraints & C_CENTROSYM)) G.y = 0.0f;
   if (a.objective == 0) {
     if (f & FLAG_MEASURED) {
       float m = 1.0f;
-      const float amp = a.amp[idx];
+      const float amp = a.amp[ai];
       if (!(a.constraints & C_MARGIN)) {
         m = __fdiv_rn(amp, cabs_ref(G));
       } else {
         const float av = cabs_ref(G);
-        const float lo = a.amp_min[idx], hi = a.amp_max[idx];
+        const float lo = a.amp_min[ai], hi = a.amp_max[ai];
         if (av < lo) m = __fdiv_rn(lo, av);
         else if (av > hi) m = __fdiv_rn(hi, av);
       }
@@ -51,13 +52,14 @@ __device__ __forceinline__ float2 project(float2 G, long long idx, const PassArg
       else G = make_float2(amp, 0.0f);
     }
   } else {
-    if (f & FLAG_MEASURED) G = a.phased_amp[idx];
+    if (f & FLAG_MEASURED) G = a.phased_amp[ai];
   }
   return G;
 }
 
 // Fourier-domain Gaussian of sp_gaussian_blur (src/image_filter.c:80-90)
-__device__ __forceinline__ float2 gauss_mult(float2 F, long long idx, const PassArgs &a) {
+__device__ __forceinline__ float2 gauss_mult(float2 F, long long gidx, const PassArgs &a) {
+  const long long idx = gidx % a.n_start;  // position within its start
   const long long nxy = (long long)a.nx * a.ny;
   const float z = (float)(idx / nxy);
   const float y = (float)((idx % nxy) / a.nx);
