@@ -134,6 +134,24 @@ int spb_blur_host(int nx, int ny, int nz, const float *in, float radius, float *
  * src/support_update.c:392-400 with the area rule :143-144 or the threshold
  * rule :175-176): updates bit 0 of flags in place. */
 int spb_support_from_blur_host(long long n, const float *blur, int type, float value, int *flags);
+/* No counterpart in the reference.  spb_support_from_blur_host without any
+ * device allocation, for callers that must not allocate device memory: a
+ * process whose HBM is reserved up front by another allocator (a framework's
+ * caching allocator, a serving loop's job pool), where a cudaMalloc of its own
+ * fails or fragments that pool, and latency-bound loops that cannot take
+ * cudaFree's device-wide synchronisation.  Same arguments, results and
+ * errors, except:
+ *  - n is at most 65536 pixels (256 x 256); larger n returns -1 with an
+ *    error naming the limit.  The device scratch is one fixed 1,122,560-byte
+ *    array in the library, shared by every call.
+ *  - the first call on a device looks that array's address up (once per
+ *    device, with the device current); make that first call before any
+ *    stream capture begins on that device.
+ *  - work runs on the legacy default stream and the call returns when it is
+ *    done.  Calls that overlap on the GPU (several host threads at once) race
+ *    on the shared scratch: serialise them.
+ * Calls no cudaMalloc, cudaFree or other allocating routine. */
+int spb_support_from_blur_noalloc(long long n, const float *blur, int type, float value, int *flags);
 
 #ifdef __cplusplus
 }

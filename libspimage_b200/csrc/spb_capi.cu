@@ -19,6 +19,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
 #include <vector>
 
 #include "spb_internal.h"
@@ -1234,4 +1235,103 @@ extern "C" int spb_support_from_blur_host(long long n, const float *blur, int ty
   cudaFree(sel);
   if (st) cudaStreamDestroy(st);
   return rc;
+}
+
+// ------------------------------------------- support mask without allocation
+// spb_support_from_blur_noalloc: the same computation as
+// spb_support_from_blur_host for callers that must not allocate device
+// memory: a process whose HBM is reserved up front by another allocator (a
+// framework's caching allocator, a serving loop's job pool), where a
+// cudaMalloc of its own fails or fragments that pool, and latency-bound loops
+// that cannot take cudaFree's device-wide synchronisation.  Its device
+// scratch is one fixed file-scope array instead of per-call allocations.
+//
+// Scratch layout (byte offsets, each 256-aligned): the selection state, then
+// blur (complex), |blur| (f32), the caller's int flags and their u8 form, each
+// sized for kNoAllocMaxPixels.  Every call shares the array and finds the
+// previous call's contents there: the selection launchers clear the state's
+// histogram, prefix and rank before use, and every other region is written
+// for the call's n pixels before it is read.  Calls that overlap on the GPU
+// (from several host threads, or on several streams) race on the array.
+namespace {
+constexpr long long kNoAllocMaxPixels = 1LL << 16;  // 256 x 256
+constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNaSel = 0;
+constexpr size_t kNaBlur = align256(kNaSel + sizeof(SelectState));
+constexpr size_t kNaAbs = align256(kNaBlur + sizeof(float2) * kNoAllocMaxPixels);
+constexpr size_t kNaIntFlags = align256(kNaAbs + sizeof(float) * kNoAllocMaxPixels);
+constexpr size_t kNaFlags = align256(kNaIntFlags + sizeof(int) * kNoAllocMaxPixels);
+constexpr size_t kNoAllocScratchBytes = align256(kNaFlags + kNoAllocMaxPixels);  // 1,122,560 bytes
+constexpr int kNoAllocMaxDevices = 64;
+static_assert(kNoAllocScratchBytes == 1122560, "scratch size is stated in spb_device.h");
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static unsigned char *g_noalloc_ptr[kNoAllocMaxDevices];
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the first call on a device does this set-up).
+static unsigned char *noalloc_scratch() {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    fail("cudaGetDevice: %s", cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    fail("device %d is beyond the %d devices spb_support_from_blur_noalloc tracks", dev, kNoAllocMaxDevices);
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      fail("cudaGetSymbolAddress(scratch) on device %d: %s", dev, cudaGetErrorString(e));
+      return nullptr;
+    }
+    g_noalloc_ptr[dev] = (unsigned char *)p;
+  }
+  return g_noalloc_ptr[dev];
+}
+
+namespace spb {
+__global__ void flags_to_u8_kernel(const int *in, uint8_t *out, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (uint8_t)(in[i] & 3);
+}
+__global__ void flags_to_int_kernel(const uint8_t *in, int *out, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+}  // namespace spb
+
+extern "C" int spb_support_from_blur_noalloc(long long n, const float *blur, int type, float value, int *flags) {
+  if (n < 1) return fail("invalid size %lld", n);
+  if (n > kNoAllocMaxPixels)
+    return fail("%lld pixels exceed the %lld-pixel limit of spb_support_from_blur_noalloc (fixed %zu-byte device "
+                "scratch); use spb_support_from_blur_host",
+                n, kNoAllocMaxPixels, kNoAllocScratchBytes);
+  if (type != SPB_SUPPORT_AREA && type != SPB_SUPPORT_THRESHOLD) return fail("unknown support update type %d", type);
+  unsigned char *s = noalloc_scratch();
+  if (!s) return -1;
+  SelectState *sel = reinterpret_cast<SelectState *>(s + kNaSel);
+  float2 *dblur = reinterpret_cast<float2 *>(s + kNaBlur);
+  float *dabs = reinterpret_cast<float *>(s + kNaAbs);
+  int *diflags = reinterpret_cast<int *>(s + kNaIntFlags);
+  uint8_t *dflags = s + kNaFlags;
+  const cudaStream_t st = 0;  // legacy default stream: no stream object is created
+  CK(cudaMemcpyAsync(dblur, blur, sizeof(float2) * (size_t)n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(diflags, flags, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st));
+  flags_to_u8_kernel<<<148, 256, 0, st>>>(diflags, dflags, n);
+  abs_kernel<<<148, 256, 0, st>>>(dblur, dabs, n);
+  CK(cudaGetLastError());
+  if (select_and_mask_on(st, sel, dabs, n, 1, type, value, dflags)) return -1;
+  flags_to_int_kernel<<<148, 256, 0, st>>>(dflags, diflags, n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(flags, diflags, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return 0;
 }
