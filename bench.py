@@ -49,6 +49,13 @@ WORKLOADS = {
         desc="single-instance RAAR 1024x1024 FP32: 5000 RAAR (beta 0.87, area support every 50, area 0.05, "
              "blur 3.0->0.7) + 200 ER",
     ),
+    "batch512": dict(
+        pattern="batch512", shape=(512, 512), stages=[("HIO", 0.9, 2000), ("ER", None, 200)], period=20,
+        area=0.05, blur={0: 3.0, 2200: 0.7}, constraints=2, starts=512,
+        desc="batched random starts: 512 reconstructions of one 512x512 FP32 pattern (128x128 blob, 1e7 photons, "
+             "beamstop 6 px), seeds 0..511, each 2000 HIO (beta 0.9) + 200 ER, area support every 20 (area 0.05, "
+             "blur 3.0->0.7)",
+    ),
     "hio256": dict(
         pattern="hio256", shape=(256, 256), stages=[("HIO", 0.9, 1000)], period=20, area=0.05,
         blur={0: 3.0, 1000: 0.7}, constraints=2,
@@ -136,7 +143,9 @@ def dist_setup():
 
 
 # ------------------------------------------------------------------ GPU arm
-def build_phaser(L, wl, amp, mask, support, seed):
+def build_phaser(L, wl, amp, mask, support, seed, starts=None, device_phases=False):
+    """Phaser for the workload; with starts > 1 a batch whose start b gets
+    device-drawn random phases keyed by seed + b."""
     ph = L.Phaser(wl["shape"])
     handles = []
     for name, beta, _ in wl["stages"]:
@@ -147,8 +156,15 @@ def build_phaser(L, wl, amp, mask, support, seed):
     ph.add_support_update(L.SpSupportArea, wl["period"], wl["blur"], wl["area"])
     ph.start()
     ph.lib.sp_phaser_set_phasing_algorithm(ph.ph, handles[0])
-    ph.set_amplitudes(amp, mask)
-    rc = ph.init_model(L.SpModelRandomPhases, seed=seed)
+    if starts is None:
+        starts = wl.get("starts", 1)
+    if starts > 1 or device_phases:
+        ph.set_starts(starts)
+        ph.set_amplitudes(amp, mask)
+        rc = ph.init_models_device(L.SpModelRandomPhases, [seed + b for b in range(starts)])
+    else:
+        ph.set_amplitudes(amp, mask)
+        rc = ph.init_model(L.SpModelRandomPhases, seed=seed)
     assert rc == 0, rc
     ph.set_support(support)
     return ph, handles
@@ -223,7 +239,8 @@ def gpu_arm(args):
     ph.profile(False)
     total_ms = replicas.max_over_ranks(float(sum(step_ms)), device="cuda")
     slots = slots_per_step(wl)
-    value = world * args.steps * slots / (total_ms / 1e3)
+    starts = wl.get("starts", 1)
+    value = world * args.steps * slots * starts / (total_ms / 1e3)
 
     # ---- end to end through the C API with host buffers
     ph.set_stream(None)
@@ -238,12 +255,21 @@ def gpu_arm(args):
     roof = None
     if per_pixel and launches:
         avg_s = ms / launches / 1e3
-        achieved = per_pixel * n / avg_s / 1e9
+        achieved = per_pixel * n * starts / avg_s / 1e9
         traffic = profiled_traffic(name, args.workload)
         roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "traffic": traffic, "algorithmic_bytes_per_launch": per_pixel * n,
+                "traffic": traffic, "algorithmic_bytes_per_launch": per_pixel * n * starts,
                 "avg_launch_us": round(avg_s * 1e6, 3)}
+
+    batched = None
+    if args.batch_steps > 0:
+        batched = batched_run(args, L, torch, world)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            batched["cpu_baseline"] = cpu_baseline(WORKLOADS["batch512"], args.cpu_sample_slots)
+            batched["cpu_baseline"]["note"] = ("the reference runs random starts one after another "
+                                               "(Reconstructor.reconstruct_loop), so its start-iterations/s "
+                                               "equal its iterations/s")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -263,10 +289,106 @@ def gpu_arm(args):
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def timed_jobs(ph, handles, wl, steps, stream, torch):
+    """Device time (ms) of `steps` whole jobs, CUDA events on the phaser's stream."""
+    evs = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run_stages(ph, handles, wl)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    return float(sum(a.elapsed_time(b) for a, b in evs))
+
+
+def batched_run(args, L, torch, world):
+    """Batched random starts (512 starts of 512x512) against the plain
+    single-start path on the same pattern and schedule; start 0 of the batch
+    and the plain run begin from the same device-drawn phases, so their final
+    Fourier errors must agree."""
+    import ctypes as C
+
+    from libspimage_b200 import replicas, synth
+
+    wl = WORKLOADS["batch512"]
+    nb = wl["starts"]
+    n = int(np.prod(wl["shape"]))
+    slots = slots_per_step(wl)
+    amp, mask, support, _ = synth.workload(wl["pattern"], seed=0)
+    stream = torch.cuda.Stream()
+    out = {"workload": wl["desc"], "starts": nb, "unit": "start-iterations/s", "steps": args.batch_steps,
+           "warmup": f"{args.batch_warm_slots} iteration slots (kernel warm-up and graph capture)",
+           "init": "random phases drawn on the device (Philox4x32-10, seeds 0..511)",
+           "l2": "inputs larger than L2 (8 GB of iterates)"}
+    res = {}
+    for label, starts in (("batched", nb), ("plain", 1)):
+        ph, handles = build_phaser(L, wl, amp, mask, support, seed=0, starts=starts, device_phases=True)
+        ph.set_stream(stream.cuda_stream)
+        rc = ph.iterate(args.batch_warm_slots)
+        assert rc == 0, rc
+        torch.cuda.synchronize()
+        l0 = ph.launch_count()
+        ms = timed_jobs(ph, handles, wl, args.batch_steps, stream, torch)
+        launches = ph.launch_count() - l0
+        ms = replicas.max_over_ranks(ms, device="cuda")
+        if starts > 1:
+            ef, _ = ph.starts_efourier()
+            e0 = float(ef[0])
+        else:
+            e0 = ph.efourier()[0]
+        res[label] = (ms, launches, e0)
+        ph.set_stream(None)
+        ph.close()
+        del ph
+        torch.cuda.empty_cache()
+    bms, blaunch, bef = res["batched"]
+    pms, _, pef = res["plain"]
+    out["value"] = round(world * args.batch_steps * slots * nb / (bms / 1e3), 1)
+    out["ms_per_step"] = round(bms / args.batch_steps, 3)
+    out["gpu_launches"] = int(blaunch)
+    out["plain"] = {"value": round(world * args.batch_steps * slots / (pms / 1e3), 1), "unit": "iterations/s",
+                    "ms_per_step": round(pms / args.batch_steps, 3),
+                    "config": "the same job for one start (the batch's start 0), same pattern and schedule"}
+    out["speedup_vs_plain"] = round(out["value"] / out["plain"]["value"], 3)
+    out["efourier_final"] = {"batched_start0": bef, "plain": pef, "equal": bef == pef}
+
+    # end to end through the C API with host buffers: amplitudes, mask and
+    # support up, device-drawn starts, the whole job, every start's model and
+    # Fourier error down
+    ph, handles = build_phaser(L, wl, amp, mask, support, seed=0, starts=nb)
+    amp_img = L.new_image(np.asarray(amp, np.complex64), mask)
+    sup_img = L.new_image(np.asarray(support, np.complex64))
+    model_img = L.new_image(np.zeros(wl["shape"], np.complex64))
+    lib = ph.lib
+    seeds = np.arange(nb, dtype=np.uint64)
+    efs = np.zeros(nb, np.float32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.batch_e2e_steps):
+        lib.sp_phaser_set_amplitudes(ph.ph, amp_img)
+        assert lib.sp_phaser_init_models_device(ph.ph, L.SpModelRandomPhases,
+                                                (seeds + 1000 * k).ctypes.data_as(C.POINTER(C.c_ulonglong))) == 0
+        assert lib.sp_phaser_init_support(ph.ph, sup_img, 0, 0.0) == 0
+        run_stages(ph, handles, wl)
+        for b in range(nb):
+            assert lib.sp_phaser_start_model(ph.ph, b, model_img) == 0
+        assert lib.sp_phaser_starts_efourier(ph.ph, efs.ctypes.data_as(C.POINTER(C.c_float)), None) == 0
+    dt = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda")
+    ph.close()
+    for img in (amp_img, sup_img, model_img):
+        L.free_image(img)
+    out["e2e"] = {"value": round(world * args.batch_e2e_steps * slots * nb / dt, 1), "unit": "start-iterations/s",
+                  "steps": args.batch_e2e_steps, "h2d_bytes_per_step": 4 * n + n + 8 * n + 8 * nb,
+                  "d2h_bytes_per_step": 8 * n * nb + 4 * nb}
+    return out
 
 
 def e2e_run(args, L, wl, amp, mask, support, rank, world, torch, dist):
@@ -418,9 +540,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="raar1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="raar1024", choices=sorted(k for k in WORKLOADS if "starts" not in WORKLOADS[k]))
     ap.add_argument("--cpu-sample-slots", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=2, help="timed whole jobs of the batched block (0: skip it)")
+    ap.add_argument("--batch-warm-slots", type=int, default=60)
+    ap.add_argument("--batch-e2e-steps", type=int, default=1)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
