@@ -82,6 +82,13 @@ static inline real sp_smap_interpolate(sp_smap *map, real x) {
   return 3 * p0y * t * pow(1 - t, 2) + p0y * pow(1 - t, 3) + 3 * p3y * (1 - t) * pow(t, 2) + p3y * pow(t, 3);
 }
 
+/* Not in the reference: exported forms of the static inline constructors
+ * above, so that a foreign-function binding has symbols to call.
+ * spb_smap_create inserts the n (key, value) pairs in order. */
+sp_smap *spb_smap_create(int n, const real *keys, const real *values);
+void spb_smap_free(sp_smap *m);
+real spb_smap_interpolate(sp_smap *m, real x);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,11 +23,13 @@ LIB = os.path.join(PKG, "libspimage_b200.so")
 
 CU_SOURCES = ["spb_kernels.cu", "spb_fast.cu", "spb_capi.cu"]
 C_SOURCES = ["host/image.c", "host/phasing.c", "host/support_update.c", "host/fft.c"]
+CXX_SOURCES = ["host/serve.cpp"]
 HEADERS = ["spb_fft.cuh", "spb_internal.h", "spb_pointwise.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xptxas", "-O3"]
 CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wno-unused-function"]
+CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall", "-Wno-unused-function", "-pthread"]
 
 
 def _nvcc() -> str:
@@ -76,8 +78,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if verbose:
                 print(" ".join(cmd))
             _run(cmd)
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc)), "include")
+    for src in CXX_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, os.path.basename(src) + ".o")
+        objs.append(o)
+        if force or _newer(o, [s] + headers):
+            cmd = ["g++"] + CXX_FLAGS + ["-I", INCLUDE, "-I", cuda_inc, "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
     if force or _newer(LIB, objs):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lm"]
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lm", "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

@@ -173,6 +173,7 @@ struct spb_ctx {
   cudaEvent_t beta_ev = nullptr;
   SelectState *sel = nullptr;  // one per start
   double *red = nullptr;       // reduce_scratch_doubles(nb)
+  unsigned long long *seeds = nullptr;  // per-start generator keys (device starts)
   int x_valid = 0, xf_valid = 0;
   float xf_gamma1 = 0.0f;
 };
@@ -426,6 +427,7 @@ extern "C" int spb_ctx_create_batch(spb_ctx **out, int nx, int ny, int nz, int n
   alloc((void **)&c->absb, nf);
   alloc((void **)&c->sel, sizeof(SelectState) * (size_t)nb);
   alloc((void **)&c->red, sizeof(double) * (size_t)reduce_scratch_doubles(nb));
+  alloc((void **)&c->seeds, sizeof(unsigned long long) * (size_t)nb);
   alloc((void **)&c->beta_base, sizeof(int));
   alloc((void **)&c->beta_dev, sizeof(float) * kBetaCap);
   if (!rc && cudaMallocHost(&c->beta_pinned, sizeof(float) * kBetaCap) != cudaSuccess) rc = fail("cudaMallocHost");
@@ -458,12 +460,31 @@ extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
 
 extern "C" int spb_ctx_starts(spb_ctx *c) { return c->nb; }
 
+// Bytes spb_ctx_create_batch and the first uses of a context allocate
+// (margins and phased amplitudes, allocated only when set, not included).
+extern "C" long long spb_ctx_footprint(int nx, int ny, int nz, int nb, int dm) {
+  if (check_dims(nx, ny, nz, nb)) return -1;
+  const long long n = (long long)nx * ny * nz, ntot = n * nb;
+  long long b = 0;
+  b += 4 * n;                                   // amp
+  b += ntot;                                    // flags
+  b += 6 * 8 * ntot;                            // g[2], X, Y, gp, T
+  b += 4 * ntot;                                // absb
+  b += (long long)sizeof(SelectState) * nb;     // sel
+  b += 8LL * reduce_scratch_doubles(nb);        // red
+  b += 8LL * nb + 4 + 4LL * kBetaCap;           // seeds, beta_base, beta table
+  b += 4 * n + n / 8 + 4096;                    // amp_line, meas_bits (upper bound)
+  b += 8LL * 2 * (nx + ny + nz) + 8LL * 3 * 65536;  // twiddles and stage tables (upper bound)
+  if (dm) b += 2 * 8 * ntot;                    // Xf, Yf
+  return b;
+}
+
 extern "C" void spb_ctx_destroy(spb_ctx *c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
                   c->gp, c->T, c->absb, c->sel, c->red, c->ax.tw, c->ay.tw, c->az.tw,
-                  c->amp_line, c->meas_bits, c->beta_dev, c->beta_base};
+                  c->amp_line, c->meas_bits, c->beta_dev, c->beta_base, c->seeds};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : c->prof.ev) cudaEventDestroy(e);
@@ -765,18 +786,14 @@ __global__ void random_phase_spectra_kernel(float2 *T, const float *amp, const u
 // Random-phase starts drawn on the device (throughput runs; the host API's
 // SpModelRandomPhases path reproduces the reference's rand() sequence instead)
 extern "C" int spb_ctx_random_phase_models(spb_ctx *c, const unsigned long long *seeds, int reset_others) {
-  unsigned long long *ds = nullptr;
-  CK(cudaMalloc(&ds, sizeof(unsigned long long) * (size_t)c->nb));
-  int rc = upload(c, ds, seeds, sizeof(unsigned long long) * (size_t)c->nb);
-  if (!rc) {
-    random_phase_spectra_kernel<<<1184, 256, 0, c->st>>>(c->T, c->amp, ds, c->n, c->nb);
-    if (cudaGetLastError() != cudaSuccess) rc = fail("random phase kernel launch failed");
-  }
-  if (!rc) rc = inverse_scaled_into_model(c);
-  if (!rc && reset_others) rc = reset_iterates(c);
-  if (!rc && cudaStreamSynchronize(c->st) != cudaSuccess) rc = fail("random phase models failed");
-  cudaFree(ds);
-  return rc;
+  if (upload(c, c->seeds, seeds, sizeof(unsigned long long) * (size_t)c->nb)) return -1;
+  random_phase_spectra_kernel<<<1184, 256, 0, c->st>>>(c->T, c->amp, c->seeds, c->n, c->nb);
+  CK(cudaGetLastError());
+  c->launches++;
+  if (inverse_scaled_into_model(c)) return -1;
+  if (reset_others && reset_iterates(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
 }
 
 namespace spb {
