@@ -271,6 +271,9 @@ def gpu_arm(args):
                                                "(Reconstructor.reconstruct_loop), so its start-iterations/s "
                                                "equal its iterations/s")
 
+    mixed = mixed_run(args, L) if args.mixed_jobs > 0 else None
+    serving = serving_run(args, L) if args.serve_window > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(wl, args.cpu_sample_slots)
@@ -290,6 +293,8 @@ def gpu_arm(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "batched": batched,
+            "mixed": mixed,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -388,6 +393,169 @@ def batched_run(args, L, torch, world):
     out["e2e"] = {"value": round(world * args.batch_e2e_steps * slots * nb / dt, 1), "unit": "start-iterations/s",
                   "steps": args.batch_e2e_steps, "h2d_bytes_per_step": 4 * n + n + 8 * n + 8 * nb,
                   "d2h_bytes_per_step": 8 * n * nb + 4 * nb}
+    return out
+
+
+# ------------------------------------------------ mixed batch and serving
+SERVE_SIZES = [((128, 128), 0.30), ((256, 256), 0.30), ((512, 512), 0.20), ((1024, 1024), 0.15),
+               ((128, 128, 128), 0.05)]
+MIXED_SIZES = [(128, 128), (192, 192), (256, 256), (384, 384), (512, 512), (1000, 1000)]
+HIO_, RAAR_, DM_, ER_ = 1, 2, 3, 4
+
+
+class PatternCache:
+    """A few seeded synthetic patterns per shape (a job reuses one of them;
+    its random starting phases come from its own seed)."""
+
+    def __init__(self, variants=2):
+        self.variants = variants
+        self.cache = {}
+
+    def get(self, shape, k):
+        from libspimage_b200 import synth
+
+        key = (tuple(shape), k % self.variants)
+        if key not in self.cache:
+            if len(shape) == 3:
+                amp, mask, sup, _ = synth.make_pattern(shape, 32, 1e8, 3, seed=key[1])
+            else:
+                n = shape[0]
+                amp, mask, sup, _ = synth.make_pattern(shape, n // 4, 1e7, n / 85.0, seed=key[1])
+            self.cache[key] = (amp, mask, (sup != 0).astype(np.int32))
+        return self.cache[key]
+
+
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs, np.float64), q)) if len(xs) else None
+
+
+def run_jobs(srv, jobs, arrivals, patterns):
+    """Submits job k at arrivals[k] seconds (relative to the first), waits for
+    all; returns per-job (submit, admit, finish, start-slots) on the server clock."""
+    ids = []
+    t0 = time.perf_counter()
+    for k, job in enumerate(jobs):
+        dt = arrivals[k] - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        amp, mask, sup = patterns.get(job["shape"], job["pattern"])
+        ids.append(srv.submit(amp, mask, sup, job["stages"], starts=job["starts"], seed=job["seed"],
+                              support_period=job["period"], area=0.05, blur=(3.0, 0.7)))
+    out = []
+    for jid, job in zip(ids, jobs):
+        info = srv.wait(jid)
+        if info["status"] != 0:
+            raise RuntimeError(f"job {jid} failed: {srv.job_error(jid)}")
+        srv.result(jid)
+        out.append((info["t_submit"], info["t_admit"], info["t_finish"], job["starts"] * info["slots"]))
+    return out
+
+
+def summarise(rows):
+    sub = np.array([r[0] for r in rows])
+    adm = np.array([r[1] for r in rows])
+    fin = np.array([r[2] for r in rows])
+    lat = fin - sub
+    span = float(fin.max() - sub.min())
+    return {"jobs": len(rows), "makespan_s": round(span, 4), "jobs_per_s": round(len(rows) / span, 3),
+            "start_iterations_per_s": round(sum(r[3] for r in rows) / span, 1),
+            "latency_p50_s": round(_pct(lat, 50), 4), "latency_p99_s": round(_pct(lat, 99), 4),
+            "queue_wait_p50_s": round(_pct(adm - sub, 50), 4), "queue_wait_p99_s": round(_pct(adm - sub, 99), 4)}
+
+
+def mixed_run(args, L):
+    """Uneven mixed batch: single-start jobs of 2-D sizes drawn from
+    {128, 192, 256, 384, 512, 1000}^2 with a random algorithm and beta, plus
+    eight 128^3 volumes, 1000 iteration slots each, all submitted at once;
+    against the same jobs run one at a time."""
+    from libspimage_b200.serve import Server
+
+    rng = np.random.default_rng(0)
+    jobs = []
+    for k in range(args.mixed_jobs):
+        shape = MIXED_SIZES[rng.integers(len(MIXED_SIZES))]
+        alg = int(rng.integers(1, 5))
+        beta = float(rng.uniform(0.7, 0.95))
+        jobs.append({"shape": shape, "stages": [(alg, beta, 1000)], "starts": 1, "seed": k, "period": 20,
+                     "pattern": k})
+    for k in range(8):
+        alg = int(rng.integers(1, 5))
+        jobs.append({"shape": (128, 128, 128), "stages": [(alg, float(rng.uniform(0.7, 0.95)), 1000)], "starts": 1,
+                     "seed": 10000 + k, "period": 20, "pattern": k})
+    patterns = PatternCache()
+    for j in jobs:
+        patterns.get(j["shape"], j["pattern"])
+    res = {}
+    for label, active in (("concurrent", args.max_active_jobs), ("one_at_a_time", 1)):
+        with Server(max_active_jobs=active, chunk_slots=100) as srv:
+            # warm-up: one short job per shape and algorithm (module loading, graph capture)
+            warm = [{"shape": sh, "stages": [(a, 0.9, 40)], "starts": 1, "seed": 0, "period": 20, "pattern": 0}
+                    for sh in MIXED_SIZES + [(128, 128, 128)] for a in (1, 2, 3, 4)]
+            run_jobs(srv, warm, [0.0] * len(warm), patterns)
+            rows = run_jobs(srv, jobs, [0.0] * len(jobs), patterns)
+            res[label] = summarise(rows)
+            res[label]["server"] = srv.stats()
+    out = {"workload": f"{args.mixed_jobs} single-start 2-D jobs, sizes U{{128,192,256,384,512,1000}}^2, algorithm "
+                       "U{ER,HIO,RAAR,DM}, beta U[0.7,0.95], plus 8 x 128^3; 1000 iteration slots each, area "
+                       "support every 20; all submitted at t=0",
+           "unit": "start-iterations/s", "value": res["concurrent"]["start_iterations_per_s"],
+           "concurrent": res["concurrent"], "one_at_a_time": res["one_at_a_time"],
+           "speedup_vs_one_at_a_time": round(res["one_at_a_time"]["makespan_s"] / res["concurrent"]["makespan_s"], 3),
+           "patterns": "2 seeded synthetic patterns per shape; phases from each job's seed (device Philox)"}
+    return out
+
+
+def serving_run(args, L):
+    """Serving: Poisson arrivals of 8-start jobs (1000 HIO + 100 ER, area
+    support every 20), sizes 128^2 .30, 256^2 .30, 512^2 .20, 1024^2 .15,
+    128^3 .05, admitted as slots and memory free up; latency = finish - arrival."""
+    from libspimage_b200.serve import Server
+
+    patterns = PatternCache()
+    for sh, _ in SERVE_SIZES:
+        patterns.get(sh, 0)
+        patterns.get(sh, 1)
+    probs = np.array([w for _, w in SERVE_SIZES])
+
+    def make_jobs(rate, window, seed):
+        rng = np.random.default_rng(seed)
+        t, arr, jobs = 0.0, [], []
+        while True:
+            t += rng.exponential(1.0 / rate)
+            if t > window:
+                break
+            sh = SERVE_SIZES[rng.choice(len(SERVE_SIZES), p=probs)][0]
+            arr.append(t)
+            jobs.append({"shape": sh, "stages": [(HIO_, 0.9, 1000), (ER_, 0.0, 100)], "starts": 8,
+                         "seed": 8 * len(jobs), "period": 20, "pattern": len(jobs)})
+        return jobs, arr
+
+    out = {"workload": "Poisson arrivals; 8 starts x (1000 HIO beta 0.9 + 100 ER) per job, area support every 20; "
+                       "sizes 128^2 .30, 256^2 .30, 512^2 .20, 1024^2 .15, 128^3 .05",
+           "unit": "jobs/s", "max_active_jobs": args.max_active_jobs}
+    with Server(max_active_jobs=args.max_active_jobs, chunk_slots=100) as srv:
+        warm, _ = make_jobs(50.0, 0.2, 99)
+        warm = [dict(j, stages=[(HIO_, 0.9, 40), (ER_, 0.0, 10)]) for j in warm]
+        warm += [{"shape": sh, "stages": [(HIO_, 0.9, 40), (ER_, 0.0, 10)], "starts": 8, "seed": 0, "period": 20,
+                  "pattern": 0} for sh, _ in SERVE_SIZES]
+        run_jobs(srv, warm, [0.0] * len(warm), patterns)
+        # offered load at the configured rate (far above capacity): queueing-dominated
+        jobs, arr = make_jobs(args.serve_rate, args.serve_window, 0)
+        over = summarise(run_jobs(srv, jobs, arr, patterns))
+        over["offered_jobs_per_s"] = args.serve_rate
+        over["window_s"] = args.serve_window
+        # a rate the server sustains: 70% of the throughput it reached above
+        rate = 0.7 * over["jobs_per_s"]
+        jobs, arr = make_jobs(rate, args.serve_sustained_window, 1)
+        sus = summarise(run_jobs(srv, jobs, arr, patterns))
+        sus["offered_jobs_per_s"] = round(rate, 3)
+        sus["window_s"] = args.serve_sustained_window
+        out["server"] = srv.stats()
+    out["overload"] = over
+    out["sustained"] = sus
+    out["value"] = over["jobs_per_s"]
+    out["latency_p50_s"] = sus["latency_p50_s"]
+    out["latency_p99_s"] = sus["latency_p99_s"]
     return out
 
 
@@ -546,6 +714,11 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=2, help="timed whole jobs of the batched block (0: skip it)")
     ap.add_argument("--batch-warm-slots", type=int, default=60)
     ap.add_argument("--batch-e2e-steps", type=int, default=1)
+    ap.add_argument("--mixed-jobs", type=int, default=256, help="2-D jobs of the mixed batch (0: skip it)")
+    ap.add_argument("--max-active-jobs", type=int, default=32)
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="offered arrivals per second")
+    ap.add_argument("--serve-window", type=float, default=1.0, help="seconds of arrivals (0: skip serving)")
+    ap.add_argument("--serve-sustained-window", type=float, default=5.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
