@@ -114,9 +114,18 @@ int make_axis(Axis &ax, int n) {
 const int kMaxAxis = 8192;
 // iterations per captured graph (even: the iterate buffers return to their roles)
 const int kGraphIters = 16;
-const int kMaxGraphs = 8;
+const int kMaxGraphs = 24;
+// calls of at most this many iterations run as one captured graph each
+const int kWholeGraphMax = 64;
 // iterations whose beta values one call can stage on the device
 const int kBetaCap = 1 << 16;
+// Pinned staging of the host->device parameter copies: the host reuses a
+// segment only after its copy has run, so it can run this many calls ahead of
+// the device before it waits.  Beta uploads of at most kSmallBeta values use
+// the small segments, longer ones the two large ones.
+const int kParamRing = 64;
+const int kSmallBeta = 256;
+const int kLargeRing = 2;
 // grid y-dimension limit of the column passes
 const int kMaxGridY = 65535;
 
@@ -127,8 +136,24 @@ struct GraphEntry {
   int alg = 0, constraints = 0, objective = 0;
   float gamma1 = 0.0f, gamma2 = 0.0f;
   int parity = 0;
+  // 0: a replayable chunk of kGraphIters iterations reading beta at
+  // *beta_base + i; n > 0: a whole call of n iterations reading beta[i]
+  int n = 0, keep_gp = 0;
   long long nodes = 0;  // kernel launches per replay
   cudaGraphExec_t exec = nullptr;
+};
+
+// Parameters of a captured support update, read by its kernels at run time.
+struct SupportParams {
+  double r2;                // pow(blur radius, 2)
+  unsigned long long rank;  // area rule: index of the threshold in descending order
+  float rel;                // threshold rule: fraction of the maximum
+  int pad;
+};
+
+struct SupportGraph {
+  cudaGraphExec_t exec = nullptr;
+  long long nodes = 0;
 };
 
 struct KernelProfile {
@@ -167,10 +192,22 @@ struct spb_ctx {
   int graph_evict = 0;
   bool use_graphs = true;
   int warm_alg[5] = {0, 0, 0, 0, 0};
-  float *beta_dev = nullptr, *beta_pinned = nullptr;
+  float *beta_dev = nullptr;
+  float *beta_pinned = nullptr;  // kLargeRing x kBetaCap, then kParamRing x kSmallBeta
   int beta_cap = 0;
   int *beta_base = nullptr;
-  cudaEvent_t beta_ev = nullptr;
+  cudaEvent_t beta_ev[kLargeRing + kParamRing] = {};
+  int beta_seg_large = 0, beta_seg_small = 0;
+  std::vector<float> beta_shadow;  // values of the last upload (the table's content in stream order)
+  int *beta_zero = nullptr;        // device 0: base of whole-call graphs
+  // captured support updates [type 1 threshold, 2 area][parity], their parameters
+  SupportGraph sup_graph[3][2];
+  int warm_sup[3] = {0, 0, 0};
+  SupportParams *spar = nullptr, *spar_pinned = nullptr;  // pinned: kParamRing entries
+  cudaEvent_t spar_ev[kParamRing] = {};
+  int spar_seg = 0;
+  bool spar_valid = false;
+  SupportParams spar_shadow{};
   SelectState *sel = nullptr;  // one per start
   double *red = nullptr;       // reduce_scratch_doubles(nb)
   unsigned long long *seeds = nullptr;  // per-start generator keys (device starts)
@@ -428,12 +465,25 @@ extern "C" int spb_ctx_create_batch(spb_ctx **out, int nx, int ny, int nz, int n
   alloc((void **)&c->sel, sizeof(SelectState) * (size_t)nb);
   alloc((void **)&c->red, sizeof(double) * (size_t)reduce_scratch_doubles(nb));
   alloc((void **)&c->seeds, sizeof(unsigned long long) * (size_t)nb);
+  alloc((void **)&c->beta_zero, sizeof(int));
+  alloc((void **)&c->spar, sizeof(SupportParams));
+  if (!rc && cudaMallocHost(&c->spar_pinned, sizeof(SupportParams) * kParamRing) != cudaSuccess)
+    rc = fail("cudaMallocHost");
+  for (int k = 0; k < kParamRing && !rc; k++) {
+    if (cudaEventCreateWithFlags(&c->spar_ev[k], cudaEventDisableTiming) != cudaSuccess) rc = fail("cudaEventCreate");
+    else if (cudaEventRecord(c->spar_ev[k], c->st) != cudaSuccess) rc = fail("cudaEventRecord");
+  }
+  if (!rc) cudaMemsetAsync(c->beta_zero, 0, sizeof(int), c->st);
   alloc((void **)&c->beta_base, sizeof(int));
   alloc((void **)&c->beta_dev, sizeof(float) * kBetaCap);
-  if (!rc && cudaMallocHost(&c->beta_pinned, sizeof(float) * kBetaCap) != cudaSuccess) rc = fail("cudaMallocHost");
+  if (!rc && cudaMallocHost(&c->beta_pinned, sizeof(float) * ((size_t)kBetaCap * kLargeRing +
+                                                                (size_t)kSmallBeta * kParamRing)) != cudaSuccess)
+    rc = fail("cudaMallocHost");
   c->beta_cap = kBetaCap;
-  if (!rc && cudaEventCreateWithFlags(&c->beta_ev, cudaEventDisableTiming) != cudaSuccess) rc = fail("cudaEventCreate");
-  if (!rc && cudaEventRecord(c->beta_ev, c->st) != cudaSuccess) rc = fail("cudaEventRecord");
+  for (int k = 0; k < kLargeRing + kParamRing && !rc; k++) {
+    if (cudaEventCreateWithFlags(&c->beta_ev[k], cudaEventDisableTiming) != cudaSuccess) rc = fail("cudaEventCreate");
+    else if (cudaEventRecord(c->beta_ev[k], c->st) != cudaSuccess) rc = fail("cudaEventRecord");
+  }
   if (!rc && make_axis(c->ax, nx)) rc = -1;
   if (!rc && make_axis(c->ay, ny)) rc = -1;
   if (!rc && make_axis(c->az, nz)) rc = -1;
@@ -484,14 +534,21 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   if (c->st) cudaStreamSynchronize(c->st);
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
                   c->gp, c->T, c->absb, c->sel, c->red, c->ax.tw, c->ay.tw, c->az.tw,
-                  c->amp_line, c->meas_bits, c->beta_dev, c->beta_base, c->seeds};
+                  c->amp_line, c->meas_bits, c->beta_dev, c->beta_base, c->seeds, c->beta_zero, c->spar};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : c->prof.ev) cudaEventDestroy(e);
   for (auto &g : c->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (c->beta_pinned) cudaFreeHost(c->beta_pinned);
-  if (c->beta_ev) cudaEventDestroy(c->beta_ev);
+  for (auto &e : c->beta_ev)
+    if (e) cudaEventDestroy(e);
+  for (auto &e : c->spar_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->spar_pinned) cudaFreeHost(c->spar_pinned);
+  for (auto &row : c->sup_graph)
+    for (auto &g : row)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
   if (c->own_st) cudaStreamDestroy(c->own_st);
   delete c;
 }
@@ -853,26 +910,32 @@ static bool same_alg(const GraphEntry &g, const spb_alg_desc *d) {
 // Graph of kGraphIters iterations reading beta from the device table at
 // *beta_base + i, followed by beta_base += kGraphIters.  kGraphIters is even,
 // so the iterate buffers return to their roles and the graph can be replayed.
-static int capture_graph(spb_ctx *c, const PassArgs &tmpl, GraphEntry &g) {
+// whole_n > 0: a graph of one whole call of whole_n iterations reading
+// beta[i] (base pointer at a device 0), the last storing gp when keep_gp.
+static int capture_graph(spb_ctx *c, const PassArgs &tmpl, GraphEntry &g, int whole_n = 0, int keep_gp = 0) {
   cudaGraph_t graph = nullptr;
   CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
   int rc = 0;
   const int cur0 = c->cur;
   const long long l0 = c->launches;
-  for (int i = 0; i < kGraphIters && !rc; i++) {
+  const int n = whole_n > 0 ? whole_n : kGraphIters;
+  for (int i = 0; i < n && !rc; i++) {
     PassArgs a = tmpl;
     a.beta_tab = c->beta_dev;
-    a.beta_base = c->beta_base;
+    a.beta_base = whole_n > 0 ? c->beta_zero : c->beta_base;
     a.beta_idx = i;
-    rc = one_iteration(c, a, nullptr);
+    rc = one_iteration(c, a, (keep_gp && i == n - 1) ? c->gp : nullptr);
   }
-  if (!rc) {
+  if (!rc && whole_n == 0) {
     add_int_kernel<<<1, 1, 0, c->st>>>(c->beta_base, kGraphIters, 0);
     if (cudaGetLastError() != cudaSuccess) rc = fail("graph capture: kernel launch failed");
+    c->launches++;
   }
   const cudaError_t ee = cudaStreamEndCapture(c->st, &graph);
   c->cur = cur0;
-  g.nodes = c->launches - l0 + 1;
+  g.nodes = c->launches - l0;
+  g.n = whole_n;
+  g.keep_gp = keep_gp;
   c->launches = l0;
   if (rc) {
     if (graph) cudaGraphDestroy(graph);
@@ -885,9 +948,10 @@ static int capture_graph(spb_ctx *c, const PassArgs &tmpl, GraphEntry &g) {
   return 0;
 }
 
-static GraphEntry *find_graph(spb_ctx *c, const spb_alg_desc *d) {
+static GraphEntry *find_graph(spb_ctx *c, const spb_alg_desc *d, int whole_n = 0, int keep_gp = 0) {
   for (auto &g : c->graphs)
-    if (g.used && same_alg(g, d) && g.parity == c->cur) return &g;
+    if (g.used && same_alg(g, d) && g.parity == c->cur && g.n == whole_n && (whole_n == 0 || g.keep_gp == keep_gp))
+      return &g;
   return nullptr;
 }
 
@@ -920,10 +984,27 @@ static GraphEntry *new_graph_slot(spb_ctx *c, const spb_alg_desc *d) {
 // address.
 static int upload_betas(spb_ctx *c, const float *beta, int n) {
   if (n > c->beta_cap) return fail("beta table holds %d iterations, %d requested", c->beta_cap, n);
-  CK(cudaEventSynchronize(c->beta_ev));
-  memcpy(c->beta_pinned, beta, sizeof(float) * (size_t)n);
-  CK(cudaMemcpyAsync(c->beta_dev, c->beta_pinned, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, c->st));
-  CK(cudaEventRecord(c->beta_ev, c->st));
+  // the table already holds these values (in stream order): nothing to copy
+  if (n <= (int)c->beta_shadow.size() && memcmp(beta, c->beta_shadow.data(), sizeof(float) * (size_t)n) == 0)
+    return 0;
+  int ev;
+  float *stage;
+  if (n <= kSmallBeta) {
+    const int seg = c->beta_seg_small;
+    c->beta_seg_small = (seg + 1) % kParamRing;
+    ev = kLargeRing + seg;
+    stage = c->beta_pinned + (size_t)kBetaCap * kLargeRing + (size_t)seg * kSmallBeta;
+  } else {
+    const int seg = c->beta_seg_large;
+    c->beta_seg_large = (seg + 1) % kLargeRing;
+    ev = seg;
+    stage = c->beta_pinned + (size_t)seg * kBetaCap;
+  }
+  CK(cudaEventSynchronize(c->beta_ev[ev]));
+  memcpy(stage, beta, sizeof(float) * (size_t)n);
+  CK(cudaMemcpyAsync(c->beta_dev, stage, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaEventRecord(c->beta_ev[ev], c->st));
+  c->beta_shadow.assign(beta, beta + n);
   return 0;
 }
 
@@ -958,6 +1039,23 @@ extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float 
   a.gamma2 = alg->gamma2;
   a.one_p_g2 = 1 + alg->gamma2;
   a.size_f = (float)(int)c->n;
+  // a short call (one support period, typically) runs as one captured graph
+  if (c->use_graphs && !c->prof.on && c->warm_alg[A] && iterations >= 2 && iterations <= kWholeGraphMax) {
+    GraphEntry *g = find_graph(c, alg, iterations, keep_gp);
+    if (!g) {
+      g = new_graph_slot(c, alg);
+      if (capture_graph(c, a, *g, iterations, keep_gp)) {
+        g->used = false;
+        return -1;
+      }
+    }
+    if (upload_betas(c, beta, iterations)) return -1;
+    CK(cudaGraphLaunch(g->exec, c->st));
+    c->launches += g->nodes;
+    c->cur ^= (iterations & 1);
+    if (A != ALG_DM) c->xf_valid = 0;
+    return 0;
+  }
   // iterations [0, ngraph) by graph replays, the rest launched directly (the
   // last one stores gp when asked)
   const int direct_tail = keep_gp ? 1 : 0;
@@ -1005,13 +1103,14 @@ extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float 
 }
 
 // blur |g1| of every start (or |img| when img != nullptr) into c->absb
-static int blur_abs(spb_ctx *c, const float2 *img, float radius) {
+static int blur_abs(spb_ctx *c, const float2 *img, float radius, const double *r2_dev = nullptr) {
   PassArgs a = base_args(c);
   a.src = img ? img : c->g[c->cur];
   a.dst = c->T;
   if (row(c, ROW_FWD_DEPHASE, a)) return -1;
   a.blur_c0 = -2. * pow(3.14159265358979323846, 2);
   a.blur_r2 = pow((double)radius, 2);
+  a.blur_r2_dev = r2_dev;
   if (middle(c, COL_BLUR, c->T, c->T, a)) return -1;
   a.src = c->T;
   a.absout = c->absb;
@@ -1024,17 +1123,23 @@ static int blur_abs(spb_ctx *c, const float2 *img, float radius) {
 // N-1 where the reference would read past the end.  Threshold rule: max|blur|
 // times value.  Then inside = |blur| > threshold.  nb starts of n pixels,
 // each with its own selection state.
+static long long area_rank(long long n, float area) {
+  long long k = (long long)(int)((float)n * area);
+  if (k >= n) k = n - 1;
+  if (k < 0) k = 0;
+  return k;
+}
+
+// dev: when set, the rank (area rule) or the relative threshold is read from
+// it at run time (captured support updates)
 static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *absv, long long n, int nb, int type,
-                              float value, uint8_t *flags) {
+                              float value, uint8_t *flags, const SupportParams *dev = nullptr) {
   if (type == SPB_SUPPORT_AREA) {
-    long long k = (long long)(int)((float)n * value);
-    if (k >= n) k = n - 1;
-    if (k < 0) k = 0;
-    CK(launch_select_kth_desc(absv, n, nb, k, sel, st));
+    CK(launch_select_kth_desc(absv, n, nb, area_rank(n, value), sel, st, dev ? &dev->rank : nullptr));
     CK(launch_mask_from_abs(absv, sel, 0.0f, 0, flags, n, nb, st));
   } else if (type == SPB_SUPPORT_THRESHOLD) {
     CK(launch_max_abs(absv, n, nb, sel, st));
-    CK(launch_mask_from_abs(absv, sel, value, 1, flags, n, nb, st));
+    CK(launch_mask_from_abs(absv, sel, value, 1, flags, n, nb, st, dev ? &dev->rel : nullptr));
   } else {
     return fail("unknown support update type %d", type);
   }
@@ -1042,16 +1147,70 @@ static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *ab
 }
 
 static int select_and_mask(spb_ctx *c, const float *absv, long long n, int nb, int type, float value,
-                           uint8_t *flags) {
+                           uint8_t *flags, const SupportParams *dev = nullptr) {
   if (prof_begin(c)) return -1;
-  if (select_and_mask_on(c->st, c->sel, absv, n, nb, type, value, flags)) return -1;
+  if (select_and_mask_on(c->st, c->sel, absv, n, nb, type, value, flags, dev)) return -1;
   c->launches += (type == SPB_SUPPORT_AREA) ? 10 : 4;
   return prof_end(c, type == SPB_SUPPORT_AREA ? 16 : 17);
 }
 
+// support-update parameters into the device block (pinned staging ring; an
+// unchanged block is not copied again)
+static int upload_support_params(spb_ctx *c, const SupportParams &p) {
+  if (c->spar_valid && memcmp(&p, &c->spar_shadow, sizeof(p)) == 0) return 0;
+  const int seg = c->spar_seg;
+  c->spar_seg = (seg + 1) % kParamRing;
+  CK(cudaEventSynchronize(c->spar_ev[seg]));
+  c->spar_pinned[seg] = p;
+  CK(cudaMemcpyAsync(c->spar, c->spar_pinned + seg, sizeof(p), cudaMemcpyHostToDevice, c->st));
+  CK(cudaEventRecord(c->spar_ev[seg], c->st));
+  c->spar_shadow = p;
+  c->spar_valid = true;
+  return 0;
+}
+
+// The support update of every start; after a first direct run of a rule, it
+// runs as a captured graph (one per rule and iterate parity) whose kernels
+// read the blur radius and rank or threshold from the device block.
 extern "C" int spb_ctx_support_update(spb_ctx *c, int type, float radius, float value) {
+  if (type != SPB_SUPPORT_AREA && type != SPB_SUPPORT_THRESHOLD) return fail("unknown support update type %d", type);
+  if (c->use_graphs && !c->prof.on && c->warm_sup[type]) {
+    SupportParams p;
+    memset(&p, 0, sizeof(p));
+    p.r2 = pow((double)radius, 2);
+    if (type == SPB_SUPPORT_AREA) p.rank = (unsigned long long)area_rank(c->n, value);
+    else p.rel = value;
+    if (upload_support_params(c, p)) return -1;
+    SupportGraph &g = c->sup_graph[type][c->cur];
+    if (!g.exec) {
+      cudaGraph_t graph = nullptr;
+      CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      const long long l0 = c->launches;
+      int rc = blur_abs(c, nullptr, radius, &c->spar->r2);
+      if (!rc) rc = select_and_mask(c, c->absb, c->n, c->nb, type, value, c->flags, c->spar);
+      const cudaError_t ee = cudaStreamEndCapture(c->st, &graph);
+      g.nodes = c->launches - l0;
+      c->launches = l0;
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ee != cudaSuccess) return fail("cudaStreamEndCapture: %s", cudaGetErrorString(ee));
+      const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        g.exec = nullptr;
+        return fail("cudaGraphInstantiate: %s", cudaGetErrorString(ie));
+      }
+    }
+    CK(cudaGraphLaunch(g.exec, c->st));
+    c->launches += g.nodes;
+    c->xf_valid = 0;
+    return 0;
+  }
   if (blur_abs(c, nullptr, radius)) return -1;
   if (select_and_mask(c, c->absb, c->n, c->nb, type, value, c->flags)) return -1;
+  c->warm_sup[type] = 1;
   c->xf_valid = 0;
   return 0;
 }

@@ -82,6 +82,7 @@ struct PassArgs {
   // blur
   double blur_c0;   // -2*pow(pi,2) (host glibc)
   double blur_r2;   // pow(radius,2)
+  const double *blur_r2_dev;  // when set, pow(radius,2) is read here (captured support updates)
   float nx_f;       // (float)nx
   float n_f;        // (float)N
 };
@@ -105,11 +106,13 @@ cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cud
 cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArgs &a, cudaStream_t st);
 // support selection and reductions; nb starts of n pixels each, start b at offset b*n
+// k_dev / rel_dev: when set, the rank k / the relative threshold is read from
+// device memory at run time instead of the value argument
 cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long long k, SelectState *state,
-                                   cudaStream_t st);
+                                   cudaStream_t st, const unsigned long long *k_dev = nullptr);
 cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st);
 cudaError_t launch_mask_from_abs(const float *absv, const SelectState *state, float rel, int use_rel, uint8_t *flags,
-                                 long long n, int nb, cudaStream_t st);
+                                 long long n, int nb, cudaStream_t st, const float *rel_dev = nullptr);
 // out[b*4 + k]; scratch of reduce_scratch_doubles(nb) doubles starting at out
 int reduce_scratch_doubles(int nb);
 cudaError_t launch_reduce_efourier(const float2 *F, const float *amp, const uint8_t *flags, long long n, int nb,

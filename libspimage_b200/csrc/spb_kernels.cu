@@ -346,13 +346,13 @@ __global__ void select_pick_kernel(SelectState *states, int shift, int last) {
   for (int j = 0; j < 8; j++) s->hist[lane * 8 + j] = 0;
 }
 
-__global__ void select_init_kernel(SelectState *states, unsigned long long rank) {
+__global__ void select_init_kernel(SelectState *states, unsigned long long rank, const unsigned long long *rank_dev) {
   SelectState *s = states + blockIdx.x;
   for (int d = threadIdx.x; d < 2048; d += blockDim.x) s->hist[d] = 0;
   if (threadIdx.x == 0) {
     s->prefix = 0;
     s->prefix_mask = 0;
-    s->rank = rank;
+    s->rank = rank_dev ? *rank_dev : rank;
     s->maxbits = 0;
   }
 }
@@ -366,8 +366,8 @@ static unsigned blocks_per_start(long long n, int nb) {
 }
 
 cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long long k, SelectState *state,
-                                   cudaStream_t st) {
-  select_init_kernel<<<nb, 256, 0, st>>>(state, (unsigned long long)k);
+                                   cudaStream_t st, const unsigned long long *k_dev) {
+  select_init_kernel<<<nb, 256, 0, st>>>(state, (unsigned long long)k, k_dev);
   const dim3 grid(blocks_per_start(n, nb), nb);
   for (int p = 0; p < 4; p++) {
     const int shift = 24 - SEL_BITS * p;
@@ -395,7 +395,7 @@ __global__ void max_finish_kernel(SelectState *states) {
 }
 
 cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st) {
-  select_init_kernel<<<nb, 256, 0, st>>>(state, 0);
+  select_init_kernel<<<nb, 256, 0, st>>>(state, 0, nullptr);
   max_abs_kernel<<<dim3(blocks_per_start(n, nb), nb), 256, 0, st>>>(absv, n, state);
   max_finish_kernel<<<nb, 1, 0, st>>>(state);
   return cudaGetLastError();
@@ -403,10 +403,10 @@ cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *
 
 // support_from_absolute_threshold (src/support_update.c:392-400): strict '>'
 __global__ void mask_kernel(const float *__restrict__ v, const SelectState *states, float rel, int use_rel,
-                            uint8_t *flags, long long n) {
+                            uint8_t *flags, long long n, const float *rel_dev) {
   const int b = blockIdx.y;
   const SelectState *s = states + b;
-  const float t = use_rel ? __fmul_rn(s->result, rel) : s->result;
+  const float t = use_rel ? __fmul_rn(s->result, rel_dev ? *rel_dev : rel) : s->result;
   v += (long long)b * n;
   flags += (long long)b * n;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -416,8 +416,8 @@ __global__ void mask_kernel(const float *__restrict__ v, const SelectState *stat
 }
 
 cudaError_t launch_mask_from_abs(const float *absv, const SelectState *state, float rel, int use_rel, uint8_t *flags,
-                                 long long n, int nb, cudaStream_t st) {
-  mask_kernel<<<dim3(blocks_per_start(n, nb), nb), 256, 0, st>>>(absv, state, rel, use_rel, flags, n);
+                                 long long n, int nb, cudaStream_t st, const float *rel_dev) {
+  mask_kernel<<<dim3(blocks_per_start(n, nb), nb), 256, 0, st>>>(absv, state, rel, use_rel, flags, n, rel_dev);
   return cudaGetLastError();
 }
 

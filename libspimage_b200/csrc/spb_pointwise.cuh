@@ -72,7 +72,8 @@ __device__ __forceinline__ float2 gauss_mult(float2 F, long long gidx, const Pas
                              __dmul_rn((double)dz, (double)dz));
   const float dist = __double2float_rn(__dsqrt_rn(s));
   const float cr = __fdiv_rn(dist, a.nx_f);
-  const double arg = __dmul_rn(__dmul_rn(a.blur_c0, __dmul_rn((double)cr, (double)cr)), a.blur_r2);
+  const double r2 = a.blur_r2_dev ? *a.blur_r2_dev : a.blur_r2;
+  const double arg = __dmul_rn(__dmul_rn(a.blur_c0, __dmul_rn((double)cr, (double)cr)), r2);
   const float m = __double2float_rn(__ddiv_rn(exp(arg), (double)a.n_f));
   return scale_cmul_dev(F, m);
 }
