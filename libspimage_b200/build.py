@@ -54,40 +54,36 @@ def _run(cmd):
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles the stale objects (in parallel) and links the library."""
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [
         os.path.join(INCLUDE, "spimage", f) for f in os.listdir(os.path.join(INCLUDE, "spimage"))
     ]
-    objs = []
-    for src in CU_SOURCES:
-        s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, os.path.basename(src) + ".o")
-        objs.append(o)
-        if force or _newer(o, [s] + headers):
-            cmd = [nvcc] + ARCH + NVCC_FLAGS + ["-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o]
-            if verbose:
-                print(" ".join(cmd))
-            _run(cmd)
-    for src in C_SOURCES:
-        s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, os.path.basename(src) + ".o")
-        objs.append(o)
-        if force or _newer(o, [s] + headers):
-            cmd = ["gcc"] + CC_FLAGS + ["-I", INCLUDE, "-c", s, "-o", o]
-            if verbose:
-                print(" ".join(cmd))
-            _run(cmd)
     cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc)), "include")
-    for src in CXX_SOURCES:
-        s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, os.path.basename(src) + ".o")
-        objs.append(o)
-        if force or _newer(o, [s] + headers):
-            cmd = ["g++"] + CXX_FLAGS + ["-I", INCLUDE, "-I", cuda_inc, "-c", s, "-o", o]
-            if verbose:
-                print(" ".join(cmd))
-            _run(cmd)
+    objs, jobs = [], []
+    for srcs, compiler in ((CU_SOURCES, "nvcc"), (C_SOURCES, "gcc"), (CXX_SOURCES, "g++")):
+        for src in srcs:
+            s = os.path.join(CSRC, src)
+            o = os.path.join(BUILD, os.path.basename(src) + ".o")
+            objs.append(o)
+            if not (force or _newer(o, [s] + headers)):
+                continue
+            if compiler == "nvcc":
+                cmd = [nvcc] + ARCH + NVCC_FLAGS + ["-I", INCLUDE, "-I", CSRC, "-c", s, "-o", o]
+            elif compiler == "gcc":
+                cmd = ["gcc"] + CC_FLAGS + ["-I", INCLUDE, "-c", s, "-o", o]
+            else:
+                cmd = ["g++"] + CXX_FLAGS + ["-I", INCLUDE, "-I", cuda_inc, "-c", s, "-o", o]
+            jobs.append(cmd)
+    if verbose:
+        for cmd in jobs:
+            print(" ".join(cmd))
+    if jobs:
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+            list(ex.map(_run, jobs))
     if force or _newer(LIB, objs):
         cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lm", "-lpthread"]
         if verbose:

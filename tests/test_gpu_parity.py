@@ -10,7 +10,9 @@ from tests._engines import AREA, DIFFMAP, ER, HIO, RAAR, STATIC, THRESHOLD, bits
 pytestmark = pytest.mark.gpu
 
 FFT_SHAPES = [(8, 8), (16, 16), (32, 32), (64, 48), (24, 40), (17, 19), (128, 128), (256, 256), (192, 384),
-              (8, 16, 12), (16, 16, 16), (5, 7, 9), (1, 64), (1000, 8), (3, 1024)]
+              (8, 16, 12), (16, 16, 16), (5, 7, 9), (1, 64), (1000, 8), (3, 1024),
+              # register kernels of the 2^a 3^b 5^c lengths (rows and columns)
+              (192, 192), (384, 40), (40, 384), (16, 1000), (1000, 24), (6, 192, 384)]
 
 
 @pytest.mark.parametrize("shape", FFT_SHAPES)
@@ -23,7 +25,7 @@ def test_fft_bit_exact(lib, oracle_mod, shape, sign):
     assert same_bits(got, want), f"max abs diff {np.abs(got - want).max()}"
 
 
-@pytest.mark.parametrize("shape", [(32, 32), (64, 48), (8, 16, 12), (128, 128)])
+@pytest.mark.parametrize("shape", [(32, 32), (64, 48), (8, 16, 12), (128, 128), (192, 192), (1000, 40)])
 @pytest.mark.parametrize("radius", [0.7, 3.0])
 def test_blur_bit_exact(lib, oracle_mod, shape, radius):
     rng = np.random.default_rng(7)
@@ -71,6 +73,9 @@ SCENARIOS = [
     ("raar_flip", (40, 30), RAAR, None, 2 | 8),
     ("hio_complex", (32, 32), HIO, None, 4),
     ("hio_real_centro", (32, 32), HIO, None, 1 | 16),
+    ("hio_area_192", (192, 192), HIO, [(AREA, 7, 2.0, 0.1)], 2),
+    ("raar_thr_1000", (24, 1000), RAAR, [(THRESHOLD, 6, 2.0, 0.2)], 2),
+    ("er_area_384", (384, 48), ER, [(AREA, 5, 1.5, 0.1)], 2),
 ]
 
 
