@@ -141,6 +141,19 @@ void sp_phaser_set_objective(SpPhaser *ph, SpPhasingObjective obj);
 int sp_support_area_update_support(SpSupportAlgorithm *alg, SpPhaser *ph);
 int sp_support_threshold_update_support(SpSupportAlgorithm *alg, SpPhaser *ph);
 int sp_support_static_update_support(SpSupportAlgorithm *alg, SpPhaser *ph);
+/* support_update.c:193-205: mask where |blurred template| exceeds the
+ * template's value at the scheduled area (mask rebuilt on the GPU) */
+int sp_support_template_update_support(SpSupportAlgorithm *alg, SpPhaser *ph);
+/* support_update.c:225-290: `size` dilations then `size` erosions of the
+ * support over the 6-neighbourhood (on the GPU) */
+int sp_support_close_update_support(SpSupportAlgorithm *alg, SpPhaser *ph);
+/* support_update.c:305-389: moves the support away from the borders of the
+ * shifted layout and its centre of mass to the origin.  The reference also
+ * Fourier-translates the phaser's cached host copy of the model, which the
+ * iterations do not read; here only the support moves.  Computed on the host
+ * from each start's support (float accumulation in pixel order, as the
+ * reference). */
+int sp_support_centre_image(SpSupportAlgorithm *alg, SpPhaser *ph);
 /* support_update.c:489-494 */
 int sp_support_array_update(SpSupportArray *array, SpPhaser *ph);
 

@@ -87,6 +87,14 @@ int spb_ctx_iterate(spb_ctx *ctx, const spb_alg_desc *alg, const float *beta, in
 int spb_ctx_support_update(spb_ctx *ctx, int type, float radius, float value);
 /* SpSupportFromPatterson (src/phasing.c:744-763) */
 int spb_ctx_support_patterson(spb_ctx *ctx, float value);
+/* sp_support_close_update_support_cpu (src/support_update.c:225-290): `size`
+ * dilations then `size` erosions of every start's support, 6-neighbourhood,
+ * no wrap-around at the borders */
+int spb_ctx_support_close(spb_ctx *ctx, int size);
+/* support bit of every start = abs_values[i] > threshold (abs_values: one
+ * start's N values on the host), as the template update's
+ * support_from_absolute_threshold (src/support_update.c:193-205,392-400) */
+int spb_ctx_support_from_abs(spb_ctx *ctx, const float *abs_values, float threshold);
 
 /* Device -> host copies: SPB_G0 (old model), SPB_G1 (model), SPB_GP (model
  * before projection), SPB_FMODEL (FFT of the model, computed on the GPU). */

@@ -5,6 +5,7 @@
  */
 #ifndef SPB_SUPPORT_UPDATE_H
 #define SPB_SUPPORT_UPDATE_H 1
+#include "image.h"
 #include "map.h"
 #ifdef __cplusplus
 extern "C" {
@@ -31,7 +32,22 @@ typedef struct {
 
 typedef struct {
   void *dummy;
+} SpSupportCentreImageParameters;
+
+typedef struct {
+  Image *blured;       /* the initial support blurred once */
+  Image *sorted;       /* the same values sorted by descending modulus */
+  sp_smap *area;       /* fraction of the initial support's area, per iteration */
+  real original_area;  /* fraction of the pixels inside the initial support */
+} SpSupportTemplateParameters;
+
+typedef struct {
+  void *dummy;
 } SpSupportStaticParameters;
+
+typedef struct {
+  int size;
+} SpSupportCloseParameters;
 
 typedef struct {
   SpSupportAlgorithmType type;
@@ -51,6 +67,12 @@ SpSupportAlgorithm *sp_support_threshold_alloc(sp_smap *blur_radius, sp_smap *th
 SpSupportAlgorithm *sp_support_area_alloc(sp_smap *blur_radius, sp_smap *area);
 /* support_update.c:95-108 */
 SpSupportAlgorithm *sp_support_static_alloc(void);
+/* support_update.c:51-84: blurs the initial support (on the GPU) and sorts it */
+SpSupportAlgorithm *sp_support_template_alloc(Image *initial_support, real blur_radius, sp_smap *area);
+/* support_update.c:110-125 */
+SpSupportAlgorithm *sp_support_close_alloc(int size);
+/* support_update.c:44-49 */
+SpSupportAlgorithm *sp_support_centre_image_alloc(void);
 /* support_update.c:458-463 */
 SpSupportArray *sp_support_array_alloc(int size, int update_period);
 /* support_update.c:471-477 */

@@ -29,7 +29,7 @@ SpSupportFromPatterson = 1
 SpEngineAutomatic, SpEngineCPU, SpEngineCUDA = 0, 1, 2
 SpPixelInsideSupport, SpPixelMeasuredAmplitude = 1, 2
 SpRecoverPhases, SpRecoverAmplitudes = 0, 1
-SpSupportThreshold, SpSupportArea, SpSupportStatic = 1, 2, 5
+SpSupportThreshold, SpSupportArea, SpSupportCentreImage, SpSupportTemplate, SpSupportStatic, SpSupportClose = 1, 2, 3, 4, 5, 6
 
 
 class sp_c3matrix(C.Structure):
@@ -101,6 +101,9 @@ def load():
         "sp_support_area_alloc": (_vp, [_vp, _vp]),
         "sp_support_threshold_alloc": (_vp, [_vp, _vp]),
         "sp_support_static_alloc": (_vp, []),
+        "sp_support_close_alloc": (_vp, [C.c_int]),
+        "sp_support_centre_image_alloc": (_vp, []),
+        "sp_support_template_alloc": (_vp, [_IMG, C.c_float, _vp]),
         "sp_support_array_init": (_vp, [_vp, C.c_int]),
         "sp_support_array_append": (None, [_vp, _vp]),
         "sp_phaser_alloc": (_PH, []),
@@ -305,6 +308,22 @@ class Phaser:
             self.sup = self.lib.sp_support_array_init(s, period)
         else:
             self.lib.sp_support_array_append(self.sup, s)
+
+    def _append_support(self, s, period):
+        if self.sup is None:
+            self.sup = self.lib.sp_support_array_init(s, period)
+        else:
+            self.lib.sp_support_array_append(self.sup, s)
+
+    def add_support_close(self, period, size):
+        self._append_support(self.lib.sp_support_close_alloc(size), period)
+
+    def add_support_centre(self, period):
+        self._append_support(self.lib.sp_support_centre_image_alloc(), period)
+
+    def add_support_template(self, period, support, blur_radius, area):
+        img = self._img(np.asarray(support, np.complex64))
+        self._append_support(self.lib.sp_support_template_alloc(img, blur_radius, smap(area)), period)
 
     def start(self, engine=SpEngineCUDA):
         rc = self.lib.sp_phaser_init(self.ph, self.alg, self.sup, engine)

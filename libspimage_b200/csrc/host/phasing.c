@@ -748,3 +748,115 @@ int spb_phaser_support_update(SpPhaser *ph, int type, real radius, real value) {
   state(ph)->flags_dev_newer = 1;
   return 0;
 }
+
+int spb_phaser_support_close(SpPhaser *ph, int size) {
+  if (sync_to_device(ph)) return -8;
+  if (spb_ctx_support_close(state(ph)->ctx, size)) return dev_error("support close");
+  state(ph)->flags_dev_newer = 1;
+  return 0;
+}
+
+int spb_phaser_support_from_abs(SpPhaser *ph, const float *abs_values, real threshold) {
+  if (sync_to_device(ph)) return -8;
+  if (spb_ctx_support_from_abs(state(ph)->ctx, abs_values, threshold)) return dev_error("template support");
+  state(ph)->flags_dev_newer = 1;
+  return 0;
+}
+
+/* sp_pixel_flags_translate_mask (src/image_util.c:3587-3611): the support bit
+ * moves by (dx,dy,dz) with wrap-around; the other bits stay in place */
+static void translate_support(int *f, int *tmp, int nx, int ny, int nz, int dx, int dy, int dz) {
+  while (dx < 0) dx += nx;
+  while (dy < 0) dy += ny;
+  while (dz < 0) dz += nz;
+  for (int x = 0; x < nx; x++)
+    for (int y = 0; y < ny; y++)
+      for (int z = 0; z < nz; z++) {
+        const int X = (x + dx) % nx, Y = (y + dy) % ny, Z = (z + dz) % nz;
+        const int v1 = f[((long)z * ny + y) * nx + x];
+        const long d = ((long)Z * ny + Y) * nx + X;
+        tmp[d] = (v1 & SpPixelInsideSupport) ? (f[d] | SpPixelInsideSupport) : (f[d] & ~SpPixelInsideSupport);
+      }
+  memcpy(f, tmp, sizeof(int) * (size_t)nx * ny * nz);
+}
+
+/* sp_support_centre_image_cpu (src/support_update.c:305-389) on one start's
+ * flags: translations that take the support off the borders of the shifted
+ * layout, then the centre of mass (src/linear_alg.c:444-473: float sums in
+ * pixel order, truncated to int) to the origin */
+static void centre_support(int *f, int *tmp, int nx, int ny, int nz) {
+#define IN(x, y, z) (f[((long)(z) * ny + (y)) * nx + (x)] & SpPixelInsideSupport)
+  if (nz == 1) {
+    for (int x = 0; x < nx; x++)
+      if (IN(x, (ny - 1) / 2, 0)) {
+        translate_support(f, tmp, nx, ny, nz, 0, (ny - 1) / 2, 0);
+        break;
+      }
+    for (int y = 0; y < ny; y++)
+      if (IN((nx - 1) / 2, y, 0)) {
+        translate_support(f, tmp, nx, ny, nz, (nx - 1) / 2, 0, 0);
+        break;
+      }
+  } else {
+    /* as in the reference, each break leaves the inner loop only */
+    for (int y = 0; y < ny; y++)
+      for (int z = 0; z < nz; z++)
+        if (IN((nx - 1) / 2, y, z)) {
+          translate_support(f, tmp, nx, ny, nz, (nx - 1) / 2, 0, 0);
+          break;
+        }
+    for (int x = 0; x < nx; x++)
+      for (int z = 0; z < nz; z++)
+        if (IN(x, (ny - 1) / 2, z)) {
+          translate_support(f, tmp, nx, ny, nz, 0, (ny - 1) / 2, 0);
+          break;
+        }
+    for (int x = 0; x < nx; x++)
+      for (int y = 0; y < ny; y++)
+        if (IN(x, y, (nz - 1) / 2)) {
+          translate_support(f, tmp, nx, ny, nz, 0, 0, (nz - 1) / 2);
+          break;
+        }
+  }
+#undef IN
+  float c[3] = {0.0f, 0.0f, 0.0f};
+  int sum = 0;
+  long i = 0;
+  for (int z = 0; z < nz; z++)
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++, i++)
+        if (f[i] & SpPixelInsideSupport) {
+          c[0] += (float)((x + (nx - 1) / 2) % nx);
+          c[1] += (float)((y + (ny - 1) / 2) % ny);
+          c[2] += (float)((z + (nz - 1) / 2) % nz);
+          sum++;
+        }
+  if (sum) {
+    c[0] /= (float)sum;
+    c[1] /= (float)sum;
+    c[2] /= (float)sum;
+    c[0] -= (float)((nx - 1) / 2);
+    c[1] -= (float)((ny - 1) / 2);
+    c[2] -= (float)((nz - 1) / 2);
+  }
+  translate_support(f, tmp, nx, ny, nz, (int)(0 - c[0]), (int)(0 - c[1]), (int)(0 - c[2]));
+}
+
+int spb_phaser_support_centre(SpPhaser *ph) {
+  if (sync_to_device(ph)) return -8;
+  spb_ctx *ctx = state(ph)->ctx;
+  const size_t n = (size_t)ph->image_size;
+  int *f = (int *)malloc(sizeof(int) * n), *tmp = (int *)calloc(n, sizeof(int));
+  int rc = 0;
+  for (int b = 0; b < sp_phaser_starts(ph) && !rc; b++) {
+    if (spb_ctx_get_start_flags(ctx, b, f)) rc = dev_error("download support");
+    if (!rc) {
+      centre_support(f, tmp, ph->nx, ph->ny, ph->nz);
+      if (spb_ctx_set_start_flags(ctx, b, f)) rc = dev_error("upload support");
+    }
+  }
+  free(f);
+  free(tmp);
+  state(ph)->flags_dev_newer = 1;
+  return rc;
+}

@@ -5,6 +5,7 @@
  * |model|, exact area quantile by radix select (or max * threshold), strict
  * '>' mask rebuild.  Schedules are evaluated with the same Bezier formula.
  */
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -13,6 +14,9 @@
 #include "spimage/spb_device.h"
 
 int spb_phaser_support_update(SpPhaser *ph, int type, real radius, real value);
+int spb_phaser_support_close(SpPhaser *ph, int size);
+int spb_phaser_support_from_abs(SpPhaser *ph, const float *abs_values, real threshold);
+int spb_phaser_support_centre(SpPhaser *ph);
 
 SpSupportAlgorithm *sp_support_threshold_alloc(sp_smap *blur_radius, sp_smap *threshold) {
   SpSupportAlgorithm *ret = (SpSupportAlgorithm *)malloc(sizeof(SpSupportAlgorithm));
@@ -42,6 +46,83 @@ SpSupportAlgorithm *sp_support_static_alloc(void) {
   ret->params = calloc(1, sizeof(SpSupportStaticParameters));
   ret->function = (void *)sp_support_static_update_support;
   return ret;
+}
+
+/* support_update.c:44-49 */
+SpSupportAlgorithm *sp_support_centre_image_alloc(void) {
+  SpSupportAlgorithm *ret = (SpSupportAlgorithm *)malloc(sizeof(SpSupportAlgorithm));
+  ret->type = SpSupportCentreImage;
+  ret->params = calloc(1, sizeof(SpSupportCentreImageParameters));
+  ret->function = (void *)sp_support_centre_image;
+  return ret;
+}
+
+/* support_update.c:110-125 */
+SpSupportAlgorithm *sp_support_close_alloc(int size) {
+  SpSupportAlgorithm *ret = (SpSupportAlgorithm *)malloc(sizeof(SpSupportAlgorithm));
+  SpSupportCloseParameters *p = (SpSupportCloseParameters *)malloc(sizeof(SpSupportCloseParameters));
+  ret->type = SpSupportClose;
+  p->size = size;
+  ret->params = p;
+  ret->function = (void *)sp_support_close_update_support;
+  return ret;
+}
+
+static float cabs_ref(Complex a) { return (float)sqrt((double)(a.im * a.im + a.re * a.re)); }
+
+static int desc_modulus(const void *pa, const void *pb) {
+  const float a = cabs_ref(*(const Complex *)pa), b = cabs_ref(*(const Complex *)pb);
+  return a < b ? 1 : (a == b ? 0 : -1);
+}
+
+/* support_update.c:51-84: the initial support blurred once (sp_gaussian_blur,
+ * on the GPU), a copy sorted by descending modulus, and the fraction of the
+ * pixels inside the initial support (accumulated in float) */
+SpSupportAlgorithm *sp_support_template_alloc(Image *initial_support, real blur_radius, sp_smap *area) {
+  SpSupportAlgorithm *ret = (SpSupportAlgorithm *)malloc(sizeof(SpSupportAlgorithm));
+  SpSupportTemplateParameters *p = (SpSupportTemplateParameters *)malloc(sizeof(SpSupportTemplateParameters));
+  ret->type = SpSupportTemplate;
+  p->blured = sp_gaussian_blur(initial_support, blur_radius);
+  p->area = area;
+  p->original_area = 0.0f;
+  const long long n = sp_image_size(initial_support);
+  for (long long i = 0; i < n; i++)
+    if (initial_support->image->data[i].re != 0.0f || initial_support->image->data[i].im != 0.0f)
+      p->original_area += 1.0f;
+  p->original_area /= (real)n;
+  p->sorted = sp_image_duplicate(p->blured, SP_COPY_DATA);
+  qsort(p->sorted->image->data, (size_t)n, sizeof(Complex), desc_modulus);
+  ret->params = p;
+  ret->function = (void *)sp_support_template_update_support;
+  return ret;
+}
+
+/* support_update.c:193-205; the index is clamped to N-1 where the reference
+ * would read past the end of the sorted values */
+int sp_support_template_update_support(SpSupportAlgorithm *alg, SpPhaser *ph) {
+  SpSupportTemplateParameters *p = (SpSupportTemplateParameters *)alg->params;
+  const real area = sp_smap_interpolate(p->area, ph->iteration);
+  const long long n = sp_image_size(p->sorted);
+  long long k = (long long)(int)((real)n * area * p->original_area);
+  if (k >= n) k = n - 1;
+  if (k < 0) k = 0;
+  const real t = cabs_ref(p->sorted->image->data[k]);
+  float *absv = (float *)malloc(sizeof(float) * (size_t)n);
+  for (long long i = 0; i < n; i++) absv[i] = cabs_ref(p->blured->image->data[i]);
+  const int rc = spb_phaser_support_from_abs(ph, absv, t);
+  free(absv);
+  return rc;
+}
+
+/* support_update.c:225-290 */
+int sp_support_close_update_support(SpSupportAlgorithm *alg, SpPhaser *ph) {
+  return spb_phaser_support_close(ph, ((SpSupportCloseParameters *)alg->params)->size);
+}
+
+/* support_update.c:305-389 */
+int sp_support_centre_image(SpSupportAlgorithm *alg, SpPhaser *ph) {
+  (void)alg;
+  return spb_phaser_support_centre(ph);
 }
 
 /* support_update.c:136-151 */

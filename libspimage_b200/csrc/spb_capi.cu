@@ -1250,6 +1250,71 @@ extern "C" int spb_ctx_support_patterson(spb_ctx *c, float value) {
   return 0;
 }
 
+namespace spb {
+// One dilation (dilate = 1) or erosion of the support bit of every start over
+// the 6-neighbourhood; neighbours outside the start's array are left out.
+// The other flag bits are copied unchanged.
+__global__ void support_morph_kernel(const uint8_t *__restrict__ src, uint8_t *__restrict__ dst, int nx, int ny,
+                                     int nz, long long n, long long ntot, int dilate) {
+  const long long nxy = (long long)nx * ny;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < ntot; k += (long long)gridDim.x * blockDim.x) {
+    const long long i = k % n;
+    const int z = (int)(i / nxy), y = (int)((i % nxy) / nx), x = (int)(i % nx);
+    const uint8_t c = src[k];
+    bool in;
+    if (dilate) {
+      in = (c & FLAG_INSIDE) || (x > 0 && (src[k - 1] & FLAG_INSIDE)) || (x < nx - 1 && (src[k + 1] & FLAG_INSIDE)) ||
+           (y > 0 && (src[k - nx] & FLAG_INSIDE)) || (y < ny - 1 && (src[k + nx] & FLAG_INSIDE)) ||
+           (z > 0 && (src[k - nxy] & FLAG_INSIDE)) || (z < nz - 1 && (src[k + nxy] & FLAG_INSIDE));
+    } else {
+      in = (c & FLAG_INSIDE) && !(x > 0 && !(src[k - 1] & FLAG_INSIDE)) &&
+           !(x < nx - 1 && !(src[k + 1] & FLAG_INSIDE)) && !(y > 0 && !(src[k - nx] & FLAG_INSIDE)) &&
+           !(y < ny - 1 && !(src[k + nx] & FLAG_INSIDE)) && !(z > 0 && !(src[k - nxy] & FLAG_INSIDE)) &&
+           !(z < nz - 1 && !(src[k + nxy] & FLAG_INSIDE));
+    }
+    dst[k] = in ? (uint8_t)(c | FLAG_INSIDE) : (uint8_t)(c & ~FLAG_INSIDE);
+  }
+}
+
+// support bit of every start = absv[i] > t (absv holds one start's values)
+__global__ void support_from_abs_kernel(const float *__restrict__ absv, float t, uint8_t *flags, long long n,
+                                        long long ntot) {
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < ntot; k += (long long)gridDim.x * blockDim.x) {
+    const uint8_t f = flags[k];
+    flags[k] = absv[k % n] > t ? (uint8_t)(f | FLAG_INSIDE) : (uint8_t)(f & ~FLAG_INSIDE);
+  }
+}
+}  // namespace spb
+
+// Support closing of every start: `size` dilations, then `size` erosions.
+// The passes alternate between the flags and a scratch copy held in the
+// |blur| buffer (an even number of passes ends in the flags).
+extern "C" int spb_ctx_support_close(spb_ctx *c, int size) {
+  if (size < 0) return fail("negative closing size %d", size);
+  uint8_t *scratch = reinterpret_cast<uint8_t *>(c->absb);
+  for (int pass = 0; pass < 2 * size; pass++) {
+    const uint8_t *src = (pass & 1) ? scratch : c->flags;
+    uint8_t *dst = (pass & 1) ? c->flags : scratch;
+    support_morph_kernel<<<1184, 256, 0, c->st>>>(src, dst, c->nx, c->ny, c->nz, c->n, c->ntot, pass < size);
+    CK(cudaGetLastError());
+    c->launches++;
+  }
+  c->xf_valid = 0;
+  return 0;
+}
+
+// Support bit of every start = abs_values[i] > threshold, abs_values one
+// start's values on the host (a fixed template).
+extern "C" int spb_ctx_support_from_abs(spb_ctx *c, const float *abs_values, float threshold) {
+  CK(cudaMemcpyAsync(c->absb, abs_values, sizeof(float) * (size_t)c->n, cudaMemcpyHostToDevice, c->st));
+  support_from_abs_kernel<<<1184, 256, 0, c->st>>>(c->absb, threshold, c->flags, c->n, c->ntot);
+  CK(cudaGetLastError());
+  c->launches++;
+  CK(cudaStreamSynchronize(c->st));
+  c->xf_valid = 0;
+  return 0;
+}
+
 static int fmodel_into_T(spb_ctx *c) {
   if (ensure_x(c)) return -1;
   return forward_rest(c, c->X, c->T);

@@ -31,7 +31,7 @@ RESTATE_SO = os.path.join(HERE, "build", "libsporacle.so")
 REF_SO = os.path.join(HERE, "_ref", "libspref.so")
 
 HIO, RAAR, DIFFMAP, ER = 1, 2, 3, 4
-SUP_THRESHOLD, SUP_AREA, SUP_STATIC = 1, 2, 5
+SUP_THRESHOLD, SUP_AREA, SUP_CENTRE, SUP_TEMPLATE, SUP_STATIC, SUP_CLOSE = 1, 2, 3, 4, 5, 6
 NO_CONSTRAINTS, REAL, POS_REAL, POS_COMPLEX, FLIP, CENTROSYM, MARGIN = 0, 1, 2, 4, 8, 16, 32
 RANDOM_PHASES, ZERO_PHASES, RANDOM_VALUES, MASKED_OUT_ZEROED = 1, 2, 4, 256
 INSIDE, MEASURED = 1, 2
@@ -89,6 +89,9 @@ def _load_restatement():
         lib.spo_set_algorithm.argtypes = [_vp, C.c_int, C.c_int, _fp, _fp, C.c_float, C.c_float, C.c_int]
         lib.spo_clear_support_updates.argtypes = [_vp]
         lib.spo_add_support_update.argtypes = [_vp, C.c_int, C.c_int, C.c_int, _fp, _fp, C.c_int, _fp, _fp]
+        lib.spo_add_support_close.argtypes = [_vp, C.c_int, C.c_int]
+        lib.spo_add_support_centre.argtypes = [_vp, C.c_int]
+        lib.spo_add_support_template.argtypes = [_vp, C.c_int, _fp, C.c_float, C.c_int, _fp, _fp]
         lib.spo_init_model.restype = C.c_int
         lib.spo_init_model.argtypes = [_vp, C.c_int, _fp]
         lib.spo_set_model.argtypes = [_vp, _fp]
@@ -156,6 +159,12 @@ def _load_reference():
         lib.sp_support_threshold_alloc.argtypes = [_vp, _vp]
         lib.sp_support_static_alloc.restype = _vp
         lib.sp_support_static_alloc.argtypes = []
+        lib.sp_support_close_alloc.restype = _vp
+        lib.sp_support_close_alloc.argtypes = [C.c_int]
+        lib.sp_support_centre_image_alloc.restype = _vp
+        lib.sp_support_centre_image_alloc.argtypes = []
+        lib.sp_support_template_alloc.restype = _vp
+        lib.sp_support_template_alloc.argtypes = [_vp, C.c_float, _vp]
         lib.sp_support_array_init.restype = _vp
         lib.sp_support_array_init.argtypes = [_vp, C.c_int]
         lib.sp_support_array_append.argtypes = [_vp, _vp]
@@ -266,6 +275,17 @@ class Restatement(_Engine):
         sk, sv = _keys_values(sel)
         self.lib.spo_add_support_update(self.ph, kind, period, len(bk), _ptr(bk), _ptr(bv), len(sk), _ptr(sk), _ptr(sv))
 
+    def add_support_close(self, period, size):
+        self.lib.spo_add_support_close(self.ph, period, size)
+
+    def add_support_centre(self, period):
+        self.lib.spo_add_support_centre(self.ph, period)
+
+    def add_support_template(self, period, support, blur_radius, area):
+        s = _f32(np.real(support)).ravel()
+        k, v = _keys_values(area)
+        self.lib.spo_add_support_template(self.ph, period, _ptr(s), blur_radius, len(k), _ptr(k), _ptr(v))
+
     def init_model(self, flags, seed=None, model=None):
         if seed is not None:
             self.lib.spo_srand(seed)
@@ -374,10 +394,25 @@ class Reference(_Engine):
             s = self.lib.sp_support_threshold_alloc(bm, sm)
         else:
             s = self.lib.sp_support_static_alloc()
+        self._append_support(s, period)
+
+    def _append_support(self, s, period):
         if self.sup is None:
             self.sup = self.lib.sp_support_array_init(s, period)
         else:
             self.lib.sp_support_array_append(self.sup, s)
+
+    def add_support_close(self, period, size):
+        self._append_support(self.lib.sp_support_close_alloc(size), period)
+
+    def add_support_centre(self, period):
+        self._append_support(self.lib.sp_support_centre_image_alloc(), period)
+
+    def add_support_template(self, period, support, blur_radius, area):
+        k, v = _keys_values(area)
+        am = self.lib.ref_smap(len(k), _ptr(k), _ptr(v))
+        img = self._image(np.asarray(support, np.complex64))
+        self._append_support(self.lib.sp_support_template_alloc(img, blur_radius, am), period)
 
     def start(self):
         """sp_phaser_init with the CPU engine; call after set_algorithm/add_support_update."""

@@ -22,6 +22,10 @@ typedef struct {
 typedef struct {
   int type;
   smap blur, sel;
+  int close_size;        /* close: dilations, then as many erosions */
+  float *tmpl_abs;       /* template: |blur of the initial support| per pixel */
+  float *tmpl_sorted;    /* template: the same values, descending */
+  float tmpl_area;       /* template: fraction of the initial support's pixels */
 } supalg;
 
 struct spo_phaser {
@@ -113,6 +117,7 @@ spo_phaser *spo_create(int nx, int ny, int nz) {
 
 void spo_destroy(spo_phaser *ph) {
   if (!ph) return;
+  spo_clear_support_updates(ph);
   free(ph->amp); free(ph->amp_min); free(ph->amp_max); free(ph->phased_amp);
   free(ph->flags); free(ph->g0); free(ph->g1); free(ph->gp);
   free(ph);
@@ -202,7 +207,13 @@ void spo_set_algorithm(spo_phaser *ph, int type, int nbeta, const float *beta_ke
 
 float spo_dm_gamma(spo_phaser *ph, int which) { return which == 1 ? ph->gamma1 : ph->gamma2; }
 
-void spo_clear_support_updates(spo_phaser *ph) { ph->nsup = 0; }
+void spo_clear_support_updates(spo_phaser *ph) {
+  for (int s = 0; s < ph->nsup; s++) {
+    free(ph->sup[s].tmpl_abs);
+    free(ph->sup[s].tmpl_sorted);
+  }
+  ph->nsup = 0;
+}
 
 /* sp_support_{threshold,area,static}_alloc + sp_support_array_{init,append},
  * src/support_update.c:7-42,95-108,458-487 */
@@ -210,9 +221,64 @@ void spo_add_support_update(spo_phaser *ph, int type, int period, int nblur, con
                             const float *blur_values, int nsel, const float *sel_keys, const float *sel_values) {
   if (ph->nsup >= MAXSUP) return;
   supalg *s = &ph->sup[ph->nsup++];
+  memset(s, 0, sizeof(*s));
   s->type = type;
   if (nblur > 0) smap_set(&s->blur, nblur, blur_keys, blur_values);
   if (nsel > 0) smap_set(&s->sel, nsel, sel_keys, sel_values);
+  ph->sup_period = period;
+}
+
+/* sp_support_close_alloc, src/support_update.c:110-125 */
+void spo_add_support_close(spo_phaser *ph, int period, int size) {
+  if (ph->nsup >= MAXSUP) return;
+  supalg *s = &ph->sup[ph->nsup++];
+  memset(s, 0, sizeof(*s));
+  s->type = SPO_SUP_CLOSE;
+  s->close_size = size;
+  ph->sup_period = period;
+}
+
+/* sp_support_centre_image_alloc, src/support_update.c:44-49 */
+void spo_add_support_centre(spo_phaser *ph, int period) {
+  if (ph->nsup >= MAXSUP) return;
+  supalg *s = &ph->sup[ph->nsup++];
+  memset(s, 0, sizeof(*s));
+  s->type = SPO_SUP_CENTRE;
+  ph->sup_period = period;
+}
+
+static int desc_float(const void *a, const void *b) {
+  const float x = *(const float *)a, y = *(const float *)b;
+  return x < y ? 1 : (x == y ? 0 : -1);
+}
+
+/* sp_support_template_alloc, src/support_update.c:51-84: the initial support
+ * blurred once; its |.| values kept in pixel order and sorted descending; the
+ * fraction of nonzero support pixels accumulated in float. */
+void spo_add_support_template(spo_phaser *ph, int period, const float *support_real, float blur_radius, int narea,
+                              const float *area_keys, const float *area_values) {
+  if (ph->nsup >= MAXSUP) return;
+  const long n = ph->n;
+  supalg *s = &ph->sup[ph->nsup++];
+  memset(s, 0, sizeof(*s));
+  s->type = SPO_SUP_TEMPLATE;
+  smap_set(&s->sel, narea, area_keys, area_values);
+  spfft_cpx *in = (spfft_cpx *)malloc(sizeof(spfft_cpx) * (size_t)n);
+  spfft_cpx *blur = (spfft_cpx *)malloc(sizeof(spfft_cpx) * (size_t)n);
+  float area = 0.0f;
+  for (long i = 0; i < n; i++) {
+    in[i].re = support_real[i];
+    in[i].im = 0.0f;
+    if (support_real[i] != 0.0f) area += 1.0f;
+  }
+  s->tmpl_area = area / (float)n;
+  spo_gaussian_blur(ph->nx, ph->ny, ph->nz, in, blur_radius, blur);
+  s->tmpl_abs = (float *)malloc(sizeof(float) * (size_t)n);
+  s->tmpl_sorted = (float *)malloc(sizeof(float) * (size_t)n);
+  for (long i = 0; i < n; i++) s->tmpl_abs[i] = s->tmpl_sorted[i] = cabsf_ref(blur[i]);
+  qsort(s->tmpl_sorted, (size_t)n, sizeof(float), desc_float);
+  free(in);
+  free(blur);
   ph->sup_period = period;
 }
 
@@ -484,10 +550,161 @@ static void support_from_threshold(spo_phaser *ph, const spfft_cpx *blur, float 
   }
 }
 
+/* sp_support_close_update_support_cpu, src/support_update.c:225-290: `size`
+ * dilations then `size` erosions of the support bit over the 6-neighbourhood;
+ * neighbours outside the array are left out. */
+static void support_close(spo_phaser *ph, int size) {
+  const int nx = ph->nx, ny = ph->ny, nz = ph->nz;
+  const long n = ph->n;
+  int *a = (int *)malloc(sizeof(int) * (size_t)n), *b = (int *)malloc(sizeof(int) * (size_t)n);
+  memcpy(a, ph->flags, sizeof(int) * (size_t)n);
+  memcpy(b, ph->flags, sizeof(int) * (size_t)n);
+  for (int pass = 0; pass < 2 * size; pass++) {
+    const int dilate = pass < size;
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          const long i = ((long)z * ny + y) * nx + x;
+          int in;
+          if (dilate) {
+            in = (a[i] & SPO_INSIDE) || (x > 0 && (a[i - 1] & SPO_INSIDE)) || (x < nx - 1 && (a[i + 1] & SPO_INSIDE)) ||
+                 (y > 0 && (a[i - nx] & SPO_INSIDE)) || (y < ny - 1 && (a[i + nx] & SPO_INSIDE)) ||
+                 (z > 0 && (a[i - (long)nx * ny] & SPO_INSIDE)) || (z < nz - 1 && (a[i + (long)nx * ny] & SPO_INSIDE));
+          } else {
+            in = !(!(a[i] & SPO_INSIDE) || (x > 0 && !(a[i - 1] & SPO_INSIDE)) ||
+                   (x < nx - 1 && !(a[i + 1] & SPO_INSIDE)) || (y > 0 && !(a[i - nx] & SPO_INSIDE)) ||
+                   (y < ny - 1 && !(a[i + nx] & SPO_INSIDE)) || (z > 0 && !(a[i - (long)nx * ny] & SPO_INSIDE)) ||
+                   (z < nz - 1 && !(a[i + (long)nx * ny] & SPO_INSIDE)));
+          }
+          b[i] = in ? (b[i] | SPO_INSIDE) : (b[i] & ~SPO_INSIDE);
+        }
+    int *t = a;
+    a = b;
+    b = t;
+  }
+  memcpy(ph->flags, a, sizeof(int) * (size_t)n);
+  free(a);
+  free(b);
+}
+
+/* sp_pixel_flags_translate_mask, src/image_util.c:3587-3611: the support bit
+ * moves by (dx,dy,dz) with wrap-around, the other bits stay in place */
+static void translate_support(spo_phaser *ph, int dx, int dy, int dz) {
+  const int nx = ph->nx, ny = ph->ny, nz = ph->nz;
+  int *t = (int *)calloc((size_t)ph->n, sizeof(int));
+  while (dx < 0) dx += nx;
+  while (dy < 0) dy += ny;
+  while (dz < 0) dz += nz;
+  for (int x = 0; x < nx; x++)
+    for (int y = 0; y < ny; y++)
+      for (int z = 0; z < nz; z++) {
+        const int X = (x + dx) % nx, Y = (y + dy) % ny, Z = (z + dz) % nz;
+        const int v1 = ph->flags[((long)z * ny + y) * nx + x];
+        const long d = ((long)Z * ny + Y) * nx + X;
+        const int v2 = ph->flags[d];
+        t[d] = (v1 & SPO_INSIDE) ? (v2 | SPO_INSIDE) : (v2 & ~SPO_INSIDE);
+      }
+  memcpy(ph->flags, t, sizeof(int) * (size_t)ph->n);
+  free(t);
+}
+
+static int inside_at(const spo_phaser *ph, int x, int y, int z) {
+  return ph->flags[((long)z * ph->ny + y) * ph->nx + x] & SPO_INSIDE;
+}
+
+/* sp_support_centre_image_cpu, src/support_update.c:305-389.  The reference
+ * also Fourier-translates ph->model, the phaser's cached host copy of the
+ * model, which the next iteration does not read: only the support moves.
+ * The centre of mass (src/linear_alg.c:444-473) is accumulated in float in
+ * pixel order and truncated to int. */
+static void support_centre(spo_phaser *ph) {
+  const int nx = ph->nx, ny = ph->ny, nz = ph->nz;
+  if (nz == 1) {
+    for (int x = 0; x < nx; x++)
+      if (inside_at(ph, x, (ny - 1) / 2, 0)) {
+        translate_support(ph, 0, (ny - 1) / 2, 0);
+        break;
+      }
+    for (int y = 0; y < ny; y++)
+      if (inside_at(ph, (nx - 1) / 2, y, 0)) {
+        translate_support(ph, (nx - 1) / 2, 0, 0);
+        break;
+      }
+  } else {
+    /* the break leaves only the inner loop */
+    for (int y = 0; y < ny; y++)
+      for (int z = 0; z < nz; z++)
+        if (inside_at(ph, (nx - 1) / 2, y, z)) {
+          translate_support(ph, (nx - 1) / 2, 0, 0);
+          break;
+        }
+    for (int x = 0; x < nx; x++)
+      for (int z = 0; z < nz; z++)
+        if (inside_at(ph, x, (ny - 1) / 2, z)) {
+          translate_support(ph, 0, (ny - 1) / 2, 0);
+          break;
+        }
+    for (int x = 0; x < nx; x++)
+      for (int y = 0; y < ny; y++)
+        if (inside_at(ph, x, y, (nz - 1) / 2)) {
+          translate_support(ph, 0, 0, (nz - 1) / 2);
+          break;
+        }
+  }
+  float c[3] = {0.0f, 0.0f, 0.0f};
+  int sum = 0;
+  long i = 0;
+  for (int z = 0; z < nz; z++)
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++, i++)
+        if (ph->flags[i] & SPO_INSIDE) {
+          c[0] += (float)((x + (nx - 1) / 2) % nx);
+          c[1] += (float)((y + (ny - 1) / 2) % ny);
+          c[2] += (float)((z + (nz - 1) / 2) % nz);
+          sum++;
+        }
+  if (sum) {
+    c[0] /= (float)sum;
+    c[1] /= (float)sum;
+    c[2] /= (float)sum;
+    c[0] -= (float)((nx - 1) / 2);
+    c[1] -= (float)((ny - 1) / 2);
+    c[2] -= (float)((nz - 1) / 2);
+  }
+  translate_support(ph, (int)(0 - c[0]), (int)(0 - c[1]), (int)(0 - c[2]));
+}
+
+/* sp_support_template_update_support_cpu, src/support_update.c:193-205: the
+ * threshold is the sorted template value at (int)(N * area * original area)
+ * (clamped to N-1 where the reference would read past the end) */
+static void support_template(spo_phaser *ph, const supalg *a) {
+  const float area = smap_at(&a->sel, ph->iteration);
+  long k = (long)(int)((float)ph->n * area * a->tmpl_area);
+  if (k >= ph->n) k = ph->n - 1;
+  if (k < 0) k = 0;
+  const float t = a->tmpl_sorted[k];
+  for (long i = 0; i < ph->n; i++) {
+    if (a->tmpl_abs[i] > t) ph->flags[i] |= SPO_INSIDE;
+    else ph->flags[i] &= ~SPO_INSIDE;
+  }
+}
+
 static void support_update(spo_phaser *ph) {
   const long n = ph->n;
   for (int s = 0; s < ph->nsup; s++) {
     const supalg *a = &ph->sup[s];
+    if (a->type == SPO_SUP_CLOSE) {
+      support_close(ph, a->close_size);
+      continue;
+    }
+    if (a->type == SPO_SUP_CENTRE) {
+      support_centre(ph);
+      continue;
+    }
+    if (a->type == SPO_SUP_TEMPLATE) {
+      support_template(ph, a);
+      continue;
+    }
     if (a->type != SPO_SUP_AREA && a->type != SPO_SUP_THRESHOLD) continue; /* static: nothing */
     const float radius = smap_at(&a->blur, ph->iteration);
     spfft_cpx *tmp = (spfft_cpx *)malloc(sizeof(spfft_cpx) * (size_t)n);

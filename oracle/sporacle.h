@@ -19,7 +19,8 @@ extern "C" {
 #endif
 
 enum { SPO_HIO = 1, SPO_RAAR = 2, SPO_DIFFMAP = 3, SPO_ER = 4 };
-enum { SPO_SUP_THRESHOLD = 1, SPO_SUP_AREA = 2, SPO_SUP_STATIC = 5 };
+enum { SPO_SUP_THRESHOLD = 1, SPO_SUP_AREA = 2, SPO_SUP_CENTRE = 3, SPO_SUP_TEMPLATE = 4, SPO_SUP_STATIC = 5,
+       SPO_SUP_CLOSE = 6 };
 enum {
   SPO_REAL = 1, SPO_POS_REAL = 2, SPO_POS_COMPLEX = 4, SPO_FLIP = 8, SPO_CENTROSYM = 16,
   SPO_MARGIN = 32
@@ -46,6 +47,10 @@ void spo_set_algorithm(spo_phaser *ph, int type, int nbeta, const float *beta_ke
 void spo_clear_support_updates(spo_phaser *ph);
 void spo_add_support_update(spo_phaser *ph, int type, int period, int nblur, const float *blur_keys,
                             const float *blur_values, int nsel, const float *sel_keys, const float *sel_values);
+void spo_add_support_close(spo_phaser *ph, int period, int size);
+void spo_add_support_centre(spo_phaser *ph, int period);
+void spo_add_support_template(spo_phaser *ph, int period, const float *support_real, float blur_radius, int narea,
+                              const float *area_keys, const float *area_values);
 int spo_init_model(spo_phaser *ph, int flags, const spfft_cpx *user_model);
 void spo_set_model(spo_phaser *ph, const spfft_cpx *model);
 int spo_iterate(spo_phaser *ph, int iterations);

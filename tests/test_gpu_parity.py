@@ -158,3 +158,41 @@ def _compare(gpu, ref, oracle_mod=None):
     else:
         assert abs(ef_g - ef_r) <= 1e-4 * abs(ef_r) + 1e-12
         assert abs(er_g - er_r) <= 1e-3 * abs(er_r) + 1e-12
+
+
+from tests._engines import MORPH_SCENARIOS, setup_morph  # noqa: E402
+
+
+@pytest.mark.parametrize("name,shape,alg,steps,shift,nit", MORPH_SCENARIOS, ids=[s[0] for s in MORPH_SCENARIOS])
+def test_close_centre_template_bit_exact(lib, oracle_mod, name, shape, alg, steps, shift, nit):
+    """closing (device morphology), centre-image (host, per start) and
+    template (device mask from the blurred template) against the oracle"""
+    ref, _ = setup_morph(oracle_mod.Restatement(shape), shape, alg, steps, shift)
+    gpu, _ = setup_morph(lib.Phaser(shape), shape, alg, steps, shift)
+    assert ref.iterate(nit) == 0
+    assert gpu.iterate(nit) == 0
+    _compare(gpu, ref)
+
+
+def test_close_centre_batched_starts(lib):
+    """the same support steps on a batch of starts equal one-start phasers"""
+    name, shape, alg, steps, shift, nit = MORPH_SCENARIOS[3]
+    seeds = [4, 9, 16]
+    amp, mask, support, _ = __import__("libspimage_b200").synth.small_pattern(shape, seed=1)
+    support = np.roll(support, shift, axis=(-2, -1))
+    batch = lib.Phaser(shape)
+    batch.set_algorithm(alg, beta=0.9, constraints=2)
+    batch.add_support_update(THRESHOLD, 5, 2.0, 0.2)
+    batch.add_support_close(5, 1)
+    batch.add_support_centre(5)
+    batch.start()
+    batch.set_starts(len(seeds))
+    batch.set_amplitudes(amp, mask)
+    assert batch.init_models(1, seeds) == 0
+    batch.set_support(support)
+    assert batch.iterate(nit) == 0
+    for b, s in enumerate(seeds):
+        one, _ = setup_morph(lib.Phaser(shape), shape, alg, steps, shift, seed=s)
+        assert one.iterate(nit) == 0
+        assert np.array_equal(batch.start_support(b), one.support())
+        assert same_bits(batch.start_model(b), one.model())

@@ -239,3 +239,21 @@ def converges(engine_factory, alg, constraints, beamstop, seed0, beta=0.8, tol=1
 @pytest.mark.parametrize("constraints,beamstop", [(2, 0), (1, 0), (4, 0), (4, 1), (2, 1)])
 def test_small_object_converges(oracle_mod, alg, constraints, beamstop):
     assert converges(oracle_mod.Restatement, alg, constraints, beamstop, seed0=17)
+
+
+from tests._engines import MORPH_SCENARIOS, setup_morph  # noqa: E402
+
+
+@pytest.mark.parametrize("name,shape,alg,steps,shift,nit", MORPH_SCENARIOS, ids=[s[0] for s in MORPH_SCENARIOS])
+def test_restatement_equals_reference_close_centre_template(oracle_mod, name, shape, alg, steps, shift, nit):
+    """closing, centre-image and template support updates of the restatement
+    against the reference's own CPU engine (src/support_update.c:44-125,
+    193-390), bit for bit"""
+    if not oracle_mod.ref_available():
+        pytest.skip("reference CPU engine not built")
+    ref, s0 = setup_morph(oracle_mod.Reference(shape), shape, alg, steps, shift)
+    res, _ = setup_morph(oracle_mod.Restatement(shape), shape, alg, steps, shift)
+    assert ref.iterate(nit) == 0 and res.iterate(nit) == 0
+    assert np.array_equal(res.support(), ref.support())
+    assert not np.array_equal(res.support(), (np.real(s0) != 0).astype(np.int32)), "support never changed"
+    assert same_bits(res.model(), ref.model())
