@@ -168,6 +168,12 @@ int sp_phaser_set_cuda_stream(SpPhaser *ph, void *stream);
  * spimage/spb_device.h), created on first use; NULL before the dimensions
  * are known. */
 void *sp_phaser_device_context(SpPhaser *ph);
+/* Not in the reference: choose the launch shapes of this phaser's device
+ * passes for its current algorithm by measurement (row lines per block,
+ * dependent launch); the reconstruction is left where it was and the choice is
+ * cached per process by shape, start count and algorithm.  Returns 0, -2
+ * without an algorithm, -8 on a device error. */
+int sp_phaser_autotune(SpPhaser *ph);
 
 /* Not in the reference: batched random starts.  The reference's
  * Reconstructor.reconstruct_loop (src/_spimage_reconstructor.py:677-740) runs

@@ -34,6 +34,8 @@ typedef struct {
   int max_active_jobs;     /* jobs on the GPU at once; 0: 32 */
   int chunk_slots;         /* iteration slots per enqueued chunk; 0: 100 */
   int chunks_ahead;        /* chunks queued per job ahead of the GPU; 0: 2 */
+  int no_autotune;         /* 1: keep the built-in launch shapes; 0: tune them (sp_phaser_autotune) for the
+                              first stage's algorithm of every new (shape, starts, algorithm) */
 } spb_server_config;
 
 enum { SPB_JOB_MAX_STAGES = 4 };

@@ -59,6 +59,24 @@ long long spb_ctx_launch_count(spb_ctx *ctx);
 int spb_ctx_profile_read(spb_ctx *ctx, int kind, long long *launches, double *total_ms);
 const char *spb_kernel_name(int kind);
 
+/* Launch-shape knobs (no reference counterpart; they change no arithmetic):
+ * SPB_TUNE_ROW_LINES = lines per block of the row passes (0: the built-in
+ * choice, 256 threads per block); SPB_TUNE_NO_PDL = 1 launches the pass
+ * kernels without programmatic dependent launch (on by default: a pass
+ * kernel stages its twiddles and the previous iterate while its predecessor
+ * finishes).  Setting a knob drops the context's captured graphs. */
+enum { SPB_TUNE_ROW_LINES = 0, SPB_TUNE_NO_PDL = 1, SPB_TUNE_KNOBS = 4 };
+int spb_ctx_set_tuning(spb_ctx *ctx, int knob, int value);
+int spb_ctx_get_tuning(spb_ctx *ctx, int knob);
+/* Autotuner (no reference counterpart): times `calls` calls of `iterations`
+ * (2..64) iterations of `alg` for each candidate launch shape (row lines per
+ * block, dependent launch on/off) and keeps the fastest; the model, iterates,
+ * support and parity are restored afterwards.  The choice is cached per
+ * process by (shape, starts, algorithm); force = 1 measures again.  best_ms
+ * (optional) receives the chosen time per iteration, -1 when taken from the
+ * cache. */
+int spb_ctx_autotune(spb_ctx *ctx, const spb_alg_desc *alg, int iterations, int calls, int force, double *best_ms);
+
 /* Host -> device copies of the phaser inputs (src/phasing.c:189-363). */
 int spb_ctx_set_amplitudes(spb_ctx *ctx, const float *amp);
 int spb_ctx_set_margins(spb_ctx *ctx, const float *amp_min, const float *amp_max);

@@ -147,6 +147,9 @@ def load():
         "spb_blur_host": (C.c_int, [C.c_int, C.c_int, C.c_int, _fp, C.c_float, _fp]),
         "spb_support_from_blur_host": (C.c_int, [C.c_longlong, _fp, C.c_int, C.c_float, _ip]),
         "sp_phaser_set_starts": (C.c_int, [_PH, C.c_int]),
+        "sp_phaser_autotune": (C.c_int, [_PH]),
+        "spb_ctx_set_tuning": (C.c_int, [_vp, C.c_int, C.c_int]),
+        "spb_ctx_get_tuning": (C.c_int, [_vp, C.c_int]),
         "sp_phaser_starts": (C.c_int, [_PH]),
         "sp_phaser_init_models": (C.c_int, [_PH, C.c_int, _ip]),
         "sp_phaser_init_models_device": (C.c_int, [_PH, C.c_int, C.POINTER(C.c_ulonglong)]),
@@ -464,6 +467,16 @@ class Phaser:
         e = np.zeros(self.starts, np.float32)
         _check(self.lib.sp_phaser_starts_support_fraction(self.ph, _p(e)), "sp_phaser_starts_support_fraction")
         return e
+
+    # -- extension: launch-shape autotuner --
+    def autotune(self):
+        _check(self.lib.sp_phaser_autotune(self.ph), "sp_phaser_autotune")
+        ctx = self.lib.sp_phaser_device_context(self.ph)
+        return {"row_lines": self.lib.spb_ctx_get_tuning(ctx, 0), "no_pdl": self.lib.spb_ctx_get_tuning(ctx, 1)}
+
+    def set_tuning(self, knob, value):
+        ctx = self.lib.sp_phaser_device_context(self.ph)
+        _check(self.lib.spb_ctx_set_tuning(ctx, knob, value), "spb_ctx_set_tuning")
 
     # -- extensions: caller stream and per-kernel timing --
     def set_stream(self, stream_handle):

@@ -636,9 +636,41 @@ int sp_phaser_init_support(SpPhaser *ph, const Image *support, int flags, real v
   return -1;
 }
 
+static void alg_desc(const SpPhaser *ph, spb_alg_desc *d, sp_smap **beta);
+
 /* `k` phasing iterations of the current algorithm on the device */
 static int run_phasing(SpPhaser *ph, int k) {
   if (k <= 0) return 0;
+  spb_alg_desc d;
+  sp_smap *beta = NULL;
+  alg_desc(ph, &d, &beta);
+  float *b = (float *)malloc(sizeof(float) * (size_t)k);
+  for (int i = 0; i < k; i++) b[i] = beta ? sp_smap_interpolate(beta, ph->iteration + i) : 0.0f;
+  const int rc = spb_ctx_iterate(state(ph)->ctx, &d, b, k, 1);
+  free(b);
+  if (rc) return dev_error("iterate");
+  ph->iteration += k;
+  return 0;
+}
+
+/* Not in the reference: launch shapes of this phaser's device passes chosen
+ * by measurement for the current algorithm (spb_ctx_autotune), over calls of
+ * one support period (or 16 iterations); the reconstruction is left where it
+ * was.  Returns 0 or -8. */
+int sp_phaser_autotune(SpPhaser *ph) {
+  if (!ph || !ph->algorithm) return -2;
+  if (sync_to_device(ph)) return -8;
+  spb_alg_desc d;
+  alg_desc(ph, &d, NULL);
+  int its = ph->sup_algorithm ? ph->sup_algorithm->update_period - 1 : 16;
+  if (its < 2) its = 2;
+  if (its > 64) its = 64;
+  if (spb_ctx_autotune(state(ph)->ctx, &d, its, 5, 0, NULL)) return dev_error("autotune");
+  return 0;
+}
+
+/* the device descriptor of the current algorithm and its beta schedule */
+static void alg_desc(const SpPhaser *ph, spb_alg_desc *dp, sp_smap **beta_out) {
   const SpPhasingAlgorithm *alg = ph->algorithm;
   spb_alg_desc d;
   memset(&d, 0, sizeof(d));
@@ -659,13 +691,8 @@ static int run_phasing(SpPhaser *ph, int k) {
   } else {
     d.constraints = ((const SpPhasingERParameters *)alg->params)->constraints;
   }
-  float *b = (float *)malloc(sizeof(float) * (size_t)k);
-  for (int i = 0; i < k; i++) b[i] = beta ? sp_smap_interpolate(beta, ph->iteration + i) : 0.0f;
-  const int rc = spb_ctx_iterate(state(ph)->ctx, &d, b, k, 1);
-  free(b);
-  if (rc) return dev_error("iterate");
-  ph->iteration += k;
-  return 0;
+  *dp = d;
+  if (beta_out) *beta_out = beta;
 }
 
 /* phasing.c:895-1024 */

@@ -279,6 +279,7 @@ int spb_server::start_job(Job &j) {
   if (sp_phaser_init_models_device(ph, SpModelRandomPhases, seeds.data()))
     return fail(std::string("initial models: ") + sp_phaser_last_error());
   if (sp_phaser_init_support(ph, s.sup_img, 0, 0)) return fail("initial support");
+  if (!cfg.no_autotune && sp_phaser_autotune(ph)) return fail(std::string("autotune: ") + sp_phaser_last_error());
   j.stage = 0;
   j.stage_left = d.stage[0].iterations;
   j.issued = 0;

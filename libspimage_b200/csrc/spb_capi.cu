@@ -19,6 +19,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -213,6 +214,7 @@ struct spb_ctx {
   unsigned long long *seeds = nullptr;  // per-start generator keys (device starts)
   int x_valid = 0, xf_valid = 0;
   float xf_gamma1 = 0.0f;
+  int tune[SPB_TUNE_KNOBS] = {};  // launch-shape choices (0: built-in)
 };
 
 namespace {
@@ -233,6 +235,8 @@ PassArgs base_args(const spb_ctx *c) {
   a.amp_line = c->amp_line;
   a.meas_bits = c->meas_bits;
   a.meas_words = c->meas_words;
+  a.row_lpb = c->tune[SPB_TUNE_ROW_LINES];
+  a.pdl = c->tune[SPB_TUNE_NO_PDL] ? 0 : 1;
   a.inv_n = (float)(1.0 / (double)c->n);
   a.nx_f = (float)c->nx;
   a.n_f = (float)c->n;
@@ -509,6 +513,37 @@ extern "C" int spb_ctx_create(spb_ctx **out, int nx, int ny, int nz) {
 }
 
 extern "C" int spb_ctx_starts(spb_ctx *c) { return c->nb; }
+
+// Captured graphs hold launch shapes and parity-dependent pointers: a change
+// of launch shape drops them, and the next call of each kind runs directly.
+static void drop_graphs(spb_ctx *c) {
+  cudaStreamSynchronize(c->st);
+  for (auto &g : c->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = GraphEntry();
+  }
+  for (auto &row : c->sup_graph)
+    for (auto &g : row) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      g = SupportGraph();
+    }
+  for (auto &w : c->warm_alg) w = 0;
+  for (auto &w : c->warm_sup) w = 0;
+}
+
+extern "C" int spb_ctx_set_tuning(spb_ctx *c, int knob, int value) {
+  if (knob < 0 || knob >= SPB_TUNE_KNOBS) return fail("unknown tuning knob %d", knob);
+  if (value < 0) return fail("negative tuning value %d", value);
+  if (c->tune[knob] != value) {
+    c->tune[knob] = value;
+    drop_graphs(c);
+  }
+  return 0;
+}
+
+extern "C" int spb_ctx_get_tuning(spb_ctx *c, int knob) {
+  return (knob >= 0 && knob < SPB_TUNE_KNOBS) ? c->tune[knob] : -1;
+}
 
 // Bytes spb_ctx_create_batch and the first uses of a context allocate
 // (margins and phased amplitudes, allocated only when set, not included).
@@ -1312,6 +1347,123 @@ extern "C" int spb_ctx_support_from_abs(spb_ctx *c, const float *abs_values, flo
   c->launches++;
   CK(cudaStreamSynchronize(c->st));
   c->xf_valid = 0;
+  return 0;
+}
+
+// ---------------------------------------------------------------- autotuner
+// Launch shapes chosen by measurement: for each candidate (row lines per
+// block, programmatic dependent launch on or off) the context runs `calls`
+// timed calls of `iterations` iterations of the given algorithm (graph
+// replays, as in production) and keeps the fastest.  The model, iterates,
+// support and parity are saved before and restored after, so tuning leaves the
+// reconstruction where it was.  Choices are cached per process by (shape,
+// starts, algorithm).
+namespace {
+struct TuneKey {
+  int nx, ny, nz, nb, alg, constraints, objective;
+  bool operator<(const TuneKey &o) const {
+    const int a[7] = {nx, ny, nz, nb, alg, constraints, objective};
+    const int b[7] = {o.nx, o.ny, o.nz, o.nb, o.alg, o.constraints, o.objective};
+    for (int i = 0; i < 7; i++)
+      if (a[i] != b[i]) return a[i] < b[i];
+    return false;
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, int>> g_tune_cache;  // -> (row lines, no-pdl)
+}  // namespace
+
+extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterations, int calls, int force,
+                                double *best_ms) {
+  if (iterations < 2 || iterations > kWholeGraphMax) return fail("autotune: 2..%d iterations per call", kWholeGraphMax);
+  if (calls < 1) calls = 1;
+  const TuneKey key{c->nx, c->ny, c->nz, c->nb, alg->algorithm, alg->constraints, alg->objective};
+  if (!force) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      if (best_ms) *best_ms = -1.0;
+      if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, it->second.first)) return -1;
+      return spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, it->second.second);
+    }
+  }
+  // save the state the timed iterations overwrite
+  const size_t nc = sizeof(float2) * (size_t)c->ntot;
+  float2 *save = nullptr;
+  uint8_t *save_flags = nullptr;
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaMalloc(&save, 4 * nc));
+  if (cudaMalloc(&save_flags, (size_t)c->ntot) != cudaSuccess) {
+    cudaFree(save);
+    return fail("autotune: no memory for the saved state");
+  }
+  const int cur0 = c->cur, xv0 = c->x_valid, xfv0 = c->xf_valid;
+  const float xfg0 = c->xf_gamma1;
+  const int knob0[2] = {c->tune[SPB_TUNE_ROW_LINES], c->tune[SPB_TUNE_NO_PDL]};
+  int rc = 0;
+  const float2 *bufs[4] = {c->g[0], c->g[1], c->gp, c->X};
+  for (int k = 0; k < 4 && !rc; k++)
+    if (cudaMemcpyAsync(save + (size_t)k * c->ntot, bufs[k], nc, cudaMemcpyDeviceToDevice, c->st) != cudaSuccess)
+      rc = fail("autotune: save failed");
+  if (!rc && cudaMemcpyAsync(save_flags, c->flags, (size_t)c->ntot, cudaMemcpyDeviceToDevice, c->st) != cudaSuccess)
+    rc = fail("autotune: save failed");
+  std::vector<float> beta((size_t)iterations, 0.9f);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    rc = fail("autotune: cudaEventCreate failed");
+  const int T = c->nx >= 16 ? c->nx / 16 : 1;
+  const int lpb_max = 256 / T > 0 ? 256 / T : 1;
+  double best = 1e30;
+  int best_lines = 0, best_nopdl = 0;
+  for (int nopdl = 0; nopdl < 2 && !rc; nopdl++) {
+    for (int lines = 0; lines <= lpb_max && !rc; lines = lines ? lines * 2 : 1) {
+      if (lines == lpb_max) continue;  // the same as the built-in choice (0)
+      if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, nopdl)) {
+        rc = -1;
+        break;
+      }
+      // warm-up: a direct call, then the graph capture
+      for (int w = 0; w < 2 && !rc; w++) rc = spb_ctx_iterate(c, alg, beta.data(), iterations, 1);
+      if (rc) break;
+      if (cudaEventRecord(e0, c->st) != cudaSuccess) rc = fail("autotune: event");
+      for (int k = 0; k < calls && !rc; k++) rc = spb_ctx_iterate(c, alg, beta.data(), iterations, 1);
+      if (!rc && cudaEventRecord(e1, c->st) != cudaSuccess) rc = fail("autotune: event");
+      float ms = 0.0f;
+      if (!rc && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        rc = fail("autotune: timing failed");
+      if (!rc && ms < best) {
+        best = ms;
+        best_lines = lines;
+        best_nopdl = nopdl;
+      }
+    }
+  }
+  // restore the state and apply the choice (or the previous knobs on error)
+  for (int k = 0; k < 4; k++)
+    cudaMemcpyAsync((void *)bufs[k], save + (size_t)k * c->ntot, nc, cudaMemcpyDeviceToDevice, c->st);
+  cudaMemcpyAsync(c->flags, save_flags, (size_t)c->ntot, cudaMemcpyDeviceToDevice, c->st);
+  cudaStreamSynchronize(c->st);
+  cudaFree(save);
+  cudaFree(save_flags);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  c->cur = cur0;
+  c->x_valid = xv0;
+  c->xf_valid = 0;  // the difference map's second transform is recomputed from the model
+  (void)xfv0;
+  (void)xfg0;
+  if (rc) {
+    spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, knob0[0]);
+    spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, knob0[1]);
+    return -1;
+  }
+  if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, best_lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, best_nopdl))
+    return -1;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = std::make_pair(best_lines, best_nopdl);
+  }
+  if (best_ms) *best_ms = best / (double)((size_t)calls * iterations);
   return 0;
 }
 

@@ -122,6 +122,35 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Programmatic dependent launch.  What a pass kernel does before this point
+// reads only data written two or more kernels earlier in the stream (twiddles,
+// the previous iterate, flags, line-major operands) and writes only shared
+// memory; the predecessor's output is read after the wait.  The successor may
+// start its own prologue once this kernel's predecessor has completed, which
+// keeps that two-kernel distance for every prologue; the release comes just
+// before the final stores, so that the successor's blocks do not take SM
+// residency from this kernel's.  Without the launch attribute both
+// instructions return at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+// called before the final stores: the successor launches during this kernel's tail
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+template <typename K, typename... Args>
+static cudaError_t launch_maybe_pdl(K k, dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                                    Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // stage-twiddle table of an N-point line into shared memory (N-1 entries)
 template <int N>
 __device__ __forceinline__ void stage_twiddles(float2 *tw_s, const float2 *__restrict__ stw) {
@@ -175,7 +204,8 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
   float2 *line = sm + N + lr * S;
   const size_t base = (size_t)row * N + t;
   stage_twiddles<N>(tw_s, stw);
-  float2 *g0_s = sm + N + lpb * S;
+  // g0 rows start on a 16-byte boundary (an even float2 offset) for the 16-byte copies
+  float2 *g0_s = sm + ((N + lpb * S + 1) & ~1);
   uint8_t *fl_s = reinterpret_cast<uint8_t *>(g0_s + lpb * N);
   if constexpr (MODE == ROW_ITER) {
     // g0 and flags of this block's rows: contiguous, copied in 16-byte chunks
@@ -187,6 +217,7 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
     const int fchunk = vrows * N / 16;
     for (int c = threadIdx.x; c < fchunk; c += blockDim.x) cp_async16(fl_s + 16 * c, fsrc + 16 * c);
   }
+  pdl_wait();
   float2 v[16];
 #pragma unroll
   for (int q = 0; q < 16; q++) {
@@ -206,11 +237,13 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
   __syncthreads();
   if constexpr (MODE == ROW_FWD || MODE == ROW_FWD_DEPHASE || MODE == ROW_FWD_F32 || MODE == ROW_FWD_SQUARE_F32) {
     reg::fft<N, false>(v, line, t, tw_s);
+    pdl_release();
     if (valid)
 #pragma unroll
       for (int q = 0; q < 16; q++) a.dst[base + T * q] = v[q];
   } else if constexpr (MODE == ROW_INV || MODE == ROW_INV_SCALE || MODE == ROW_INV_ABS) {
     reg::fft<N, true>(v, line, t, tw_s);
+    pdl_release();
     if (valid)
 #pragma unroll
       for (int q = 0; q < 16; q++) {
@@ -248,6 +281,7 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
       v[q] = g;
     }
     reg::fft<N, false>(v, line, t, tw_s);
+    pdl_release();
     if (valid)
 #pragma unroll
       for (int q = 0; q < 16; q++) a.dst[base + T * q] = v[q];
@@ -291,6 +325,7 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
   }
   const size_t lbase = (size_t)(a.outer0 + blockIdx.y) * a.ostride + col + (size_t)t * a.estride;
   const size_t qstride = (size_t)T * a.estride;
+  pdl_wait();
   float2 v[16];
 #pragma unroll
   for (int q = 0; q < 16; q++) {
@@ -334,6 +369,7 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
     }
     reg::fft<N, true>(v, line, t, tw_s);
   }
+  pdl_release();
   if (valid)
 #pragma unroll
     for (int q = 0; q < 16; q++) a.dst[lbase + q * qstride] = v[q];
@@ -351,17 +387,20 @@ static cudaError_t set_smem(K k, size_t smem, bool &done) {
 template <int N, int MODE>
 static cudaError_t row_fast_launch(const LinePlan &px, const PassArgs &a, cudaStream_t st) {
   constexpr int T = N / 16;
-  constexpr int LPB = (256 / T) > 0 ? (256 / T) : 1;
+  constexpr int LPB_MAX = (256 / T) > 0 ? (256 / T) : 1;  // 256 threads per block at most
+  const int LPB = (a.row_lpb > 0 && a.row_lpb < LPB_MAX) ? a.row_lpb : LPB_MAX;
   const long long nrows = a.n / N;
-  size_t smem = (size_t)(N + LPB * (N + N / 16)) * sizeof(float2);
+  size_t smem = (size_t)((N + LPB * (N + N / 16) + 1) & ~1) * sizeof(float2);
   if (MODE == ROW_ITER) smem += (size_t)LPB * N * (sizeof(float2) + 1);
   auto k = row_fast_kernel<N, MODE>;
   static bool done = false;
+  static size_t done_smem = 0;
+  if (smem > done_smem) done = false;
   cudaError_t e = set_smem(k, smem, done);
   if (e != cudaSuccess) return e;
+  if (smem > done_smem) done_smem = smem;
   const long long grid = (nrows + LPB - 1) / LPB;
-  k<<<(unsigned)grid, LPB * T, smem, st>>>(a, px.stw, (int)nrows);
-  return cudaGetLastError();
+  return launch_maybe_pdl(k, dim3((unsigned)grid), dim3(LPB * T), smem, st, a.pdl != 0, a, px.stw, (int)nrows);
 }
 
 template <int N>
@@ -386,8 +425,7 @@ static cudaError_t col_fast_launch_p(const LinePlan &pl, const PassArgs &a, cuda
   if (e != cudaSuccess) return e;
   if (smem > done_smem) done_smem = smem;
   dim3 grid((a.ncols + C - 1) / C, a.nouter);
-  k<<<grid, C * T, smem, st>>>(a, pl.stw);
-  return cudaGetLastError();
+  return launch_maybe_pdl(k, grid, dim3(C * T), smem, st, a.pdl != 0, a, pl.stw);
 }
 
 template <int N, int MODE>

@@ -68,6 +68,10 @@ struct PassArgs {
   const float *amp_line;
   const uint32_t *meas_bits;
   int meas_words;
+  // launch shape: lines per block of the row pass (0: the built-in choice)
+  int row_lpb;
+  // 1: launch the register pass kernels with programmatic dependent launch
+  int pdl;
   // scalars
   int alg, constraints, objective;
   float beta, one_m2b, inv_n;

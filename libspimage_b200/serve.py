@@ -19,7 +19,7 @@ MAX_STAGES = 4
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_double), ("max_active_jobs", C.c_int), ("chunk_slots", C.c_int),
-                ("chunks_ahead", C.c_int)]
+                ("chunks_ahead", C.c_int), ("no_autotune", C.c_int)]
 
 
 class JobStage(C.Structure):
@@ -73,9 +73,10 @@ def _shape3(shape):
 class Server:
     """A running reconstruction server (one native worker thread)."""
 
-    def __init__(self, hbm_budget_bytes=0.0, max_active_jobs=0, chunk_slots=0, chunks_ahead=0):
+    def __init__(self, hbm_budget_bytes=0.0, max_active_jobs=0, chunk_slots=0, chunks_ahead=0, autotune=True):
         self.lib = _bind(load())
-        cfg = ServerConfig(float(hbm_budget_bytes), int(max_active_jobs), int(chunk_slots), int(chunks_ahead))
+        cfg = ServerConfig(float(hbm_budget_bytes), int(max_active_jobs), int(chunk_slots), int(chunks_ahead),
+                           0 if autotune else 1)
         h = C.c_void_p()
         if self.lib.spb_server_create(C.byref(h), C.byref(cfg)) != 0:
             raise RuntimeError(self.lib.spb_server_last_error().decode())
