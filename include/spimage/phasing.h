@@ -191,7 +191,9 @@ int sp_phaser_set_starts(SpPhaser *ph, int starts);
 int sp_phaser_starts(const SpPhaser *ph);
 /* Starting models drawn per start on the host exactly as sp_phaser_init_model
  * draws them after sp_srand(seeds[b]) (flags as there, user model not
- * allowed), so start b reproduces a one-start run seeded with seeds[b]. */
+ * allowed), so start b reproduces a one-start run seeded with seeds[b].  With
+ * seeds NULL the starts are drawn one after another from the current rand()
+ * stream, as nb consecutive sp_phaser_init_model calls would draw them. */
 int sp_phaser_init_models(SpPhaser *ph, int flags, const int *seeds);
 /* Random-phase starting models drawn on the device (Philox4x32-10 keyed by
  * seeds[b]); for throughput runs that do not need the reference's rand()
@@ -202,6 +204,8 @@ int sp_phaser_init_models_device(SpPhaser *ph, int flags, const unsigned long lo
 int sp_phaser_start_model(SpPhaser *ph, int start, Image *out);
 int sp_phaser_start_support(SpPhaser *ph, int start, Image *out);
 int sp_phaser_start_model_before_projection(SpPhaser *ph, int start, Image *out);
+/* Start b's Fourier-space model (FFT of its model), as sp_phaser_fmodel. */
+int sp_phaser_start_fmodel(SpPhaser *ph, int start, Image *out);
 /* Per-start metrics into out[starts] (FcFo may be NULL). */
 int sp_phaser_starts_efourier(SpPhaser *ph, real *out, real *FcFo);
 int sp_phaser_starts_ereal(SpPhaser *ph, real *out);

@@ -156,6 +156,8 @@ def load():
         "sp_phaser_start_model": (C.c_int, [_PH, C.c_int, _IMG]),
         "sp_phaser_start_support": (C.c_int, [_PH, C.c_int, _IMG]),
         "sp_phaser_start_model_before_projection": (C.c_int, [_PH, C.c_int, _IMG]),
+        "sp_phaser_start_fmodel": (C.c_int, [_PH, C.c_int, _IMG]),
+        "sp_phaser_set_support_algorithm": (C.c_int, [_PH, _vp]),
         "sp_phaser_starts_efourier": (C.c_int, [_PH, _fp, _fp]),
         "sp_phaser_starts_ereal": (C.c_int, [_PH, _fp]),
         "sp_phaser_starts_support_fraction": (C.c_int, [_PH, _fp]),
@@ -425,7 +427,11 @@ class Phaser:
     def starts(self):
         return int(self.lib.sp_phaser_starts(self.ph))
 
-    def init_models(self, flags, seeds):
+    def init_models(self, flags, seeds=None):
+        """seeds[b] seeds start b; None draws the starts one after another
+        from the current rand() stream"""
+        if seeds is None:
+            return self.lib.sp_phaser_init_models(self.ph, flags, None)
         s = np.ascontiguousarray(seeds, dtype=np.int32)
         assert s.size == self.starts
         return self.lib.sp_phaser_init_models(self.ph, flags, _p(s, _ip))
@@ -445,6 +451,9 @@ class Phaser:
 
     def start_model(self, b):
         return self._start_image(self.lib.sp_phaser_start_model, b)
+
+    def start_fmodel(self, b):
+        return self._start_image(self.lib.sp_phaser_start_fmodel, b)
 
     def start_model_before_projection(self, b):
         return self._start_image(self.lib.sp_phaser_start_model_before_projection, b)

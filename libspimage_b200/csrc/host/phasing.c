@@ -495,7 +495,7 @@ int sp_phaser_init_models(SpPhaser *ph, int flags, const int *seeds) {
     /* nb Fourier-space starts, transformed together on the device */
     float *all = (float *)malloc(sizeof(float) * 2 * n * (size_t)nb);
     for (int b = 0; b < nb; b++) {
-      sp_srand(seeds[b]);
+      if (seeds) sp_srand(seeds[b]);
       draw_start(ph, flags, m);
       memcpy(all + 2 * n * (size_t)b, m->image->data, sizeof(float) * 2 * n);
     }
@@ -503,7 +503,7 @@ int sp_phaser_init_models(SpPhaser *ph, int flags, const int *seeds) {
     free(all);
   } else {
     for (int b = 0; b < nb && !rc; b++) {
-      sp_srand(seeds[b]);
+      if (seeds) sp_srand(seeds[b]);
       draw_start(ph, flags, m);
       rc = spb_ctx_set_start_model(ctx, b, (const float *)m->image->data, b == 0);
     }
@@ -554,6 +554,11 @@ int sp_phaser_start_model(SpPhaser *ph, int start, Image *out) { return start_im
 
 int sp_phaser_start_model_before_projection(SpPhaser *ph, int start, Image *out) {
   return start_image(ph, start, out, SPB_GP);
+}
+
+int sp_phaser_start_fmodel(SpPhaser *ph, int start, Image *out) {
+  if (sync_to_device(ph)) return -8;
+  return start_image(ph, start, out, SPB_FMODEL);
 }
 
 int sp_phaser_start_support(SpPhaser *ph, int start, Image *out) {
