@@ -232,6 +232,76 @@ __device__ void stage_generic(const float2 *__restrict__ x, float2 *__restrict__
   }
 }
 
+// ------------------------------------------- compile-time plans (2,3,4,5,8,16)
+// The canonical radix plan of a length known at compile time: 16s first, then
+// one 8/4/2 (a trailing 2 after a 16 turns that 16 into 8*4), then 3s and 5s;
+// -1 when another prime remains.
+__host__ __device__ constexpr int ct_plan(int n, int *r) {
+  int k = 0, m = n, n16 = 0;
+  while (m % 16 == 0) { r[k++] = 16; m /= 16; n16++; }
+  if (m % 8 == 0) { r[k++] = 8; m /= 8; }
+  else if (m % 4 == 0) { r[k++] = 4; m /= 4; }
+  else if (m % 2 == 0) {
+    if (n16 > 0) { r[k - 1] = 8; r[k++] = 4; }
+    else r[k++] = 2;
+    m /= 2;
+  }
+  while (m % 3 == 0) { r[k++] = 3; m /= 3; }
+  while (m % 5 == 0) { r[k++] = 5; m /= 5; }
+  return m > 1 ? -1 : k;
+}
+__host__ __device__ constexpr int ct_plan_len(int n) {
+  int r[32] = {};
+  return ct_plan(n, r);
+}
+__host__ __device__ constexpr int ct_plan_radix(int n, int s) {
+  int r[32] = {};
+  ct_plan(n, r);
+  return r[s];
+}
+
+// the largest number of butterflies of any stage: threads per line that give
+// every thread at most one butterfly per stage
+__host__ __device__ constexpr int ct_max_butterflies(int n) {
+  int r[32] = {};
+  const int k = ct_plan(n, r);
+  int m = 0;
+  for (int s = 0; s < k; s++) m = (n / r[s] > m) ? n / r[s] : m;
+  return m;
+}
+
+// The stages of stage_fixed with the plan, the strides and the divisions known
+// at compile time; twiddles from the per-stage table ([stage][m-1][k], the
+// same float values as tw[m*k*tstep]), so the arithmetic is unchanged.
+template <int N, int S, int NS, bool INV>
+struct CtStages {
+  static __device__ float2 *run(float2 *x, float2 *y, const float2 *__restrict__ stw, int es, int t0, int tn) {
+    constexpr int R = ct_plan_radix(N, S);
+    constexpr int NB = N / R;
+    for (int b = t0; b < NB; b += tn) {
+      const int k = b % NS;
+      float2 a[R];
+#pragma unroll
+      for (int m = 0; m < R; m++) a[m] = x[(b + m * NB) * es];
+      if (NS > 1 && k) {
+#pragma unroll
+        for (int m = 1; m < R; m++) {
+          float2 w = __ldg(stw + (m - 1) * NS + k);
+          if (INV) w.y = -w.y;
+          a[m] = cmulw(a[m], w.x, w.y);
+        }
+      }
+      bfly<R, INV>(a);
+      const int base = (b / NS) * NS * R + k;
+#pragma unroll
+      for (int m = 0; m < R; m++) y[(base + m * NS) * es] = a[m];
+    }
+    __syncthreads();
+    if constexpr (S + 1 < ct_plan_len(N)) return CtStages<N, S + 1, NS * R, INV>::run(y, x, stw + (R - 1) * NS, es, t0, tn);
+    else return y;
+  }
+};
+
 // Runs every stage of a line transform between two staging buffers.  All
 // threads of the block must call it (it synchronises the block between
 // stages).  Returns the buffer holding the result.
@@ -259,4 +329,13 @@ __device__ float2 *line_fft(float2 *bufA, float2 *bufB, const LinePlan &p, int e
   return x;
 }
 
+}  // namespace spb
+
+namespace spb {
+// line_fft with the plan fixed at compile time when NC > 0
+template <bool INV, int NC>
+__device__ __forceinline__ float2 *line_fft_sel(float2 *bufA, float2 *bufB, const LinePlan &p, int es, int t0, int tn) {
+  if constexpr (NC > 0) return CtStages<NC, 0, 1, INV>::run(bufA, bufB, p.stw, es, t0, tn);
+  else return line_fft<INV>(bufA, bufB, p, es, t0, tn);
+}
 }  // namespace spb

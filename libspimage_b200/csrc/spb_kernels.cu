@@ -17,7 +17,7 @@
 namespace spb {
 
 // ---------------------------------------------------------------- row pass
-template <int MODE>
+template <int MODE, int NC>
 __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, int tpr, int rpb, long long nrows) {
   extern __shared__ float2 smem[];
   const int n = px.n;
@@ -56,11 +56,11 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
 
   if constexpr (MODE == ROW_FWD || MODE == ROW_FWD_DEPHASE || MODE == ROW_FWD_F32 || MODE == ROW_FWD_SQUARE_F32 ||
                 MODE == ROW_DM_F1_FWD) {
-    float2 *r = line_fft<false>(A, B, px, 1, t, tpr);
+    float2 *r = line_fft_sel<false, NC>(A, B, px, 1, t, tpr);
     if (valid)
       for (int i = t; i < n; i += tpr) a.dst[base + i] = r[i];
   } else if constexpr (MODE == ROW_INV || MODE == ROW_INV_SCALE || MODE == ROW_INV_ABS) {
-    float2 *r = line_fft<true>(A, B, px, 1, t, tpr);
+    float2 *r = line_fft_sel<true, NC>(A, B, px, 1, t, tpr);
     if (valid) {
       for (int i = t; i < n; i += tpr) {
         if constexpr (MODE == ROW_INV) a.dst[base + i] = r[i];
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
   } else if constexpr (MODE == ROW_ITER) {
     const float beta = iter_beta(a);
     const float one_m2b = fsub(1.0f, fmul(2.0f, beta));  // 1 - 2*beta in float, as the reference
-    float2 *r = line_fft<true>(A, B, px, 1, t, tpr);
+    float2 *r = line_fft_sel<true, NC>(A, B, px, 1, t, tpr);
     for (int i = t; i < n; i += tpr) {
       float2 g = make_float2(0.0f, 0.0f);
       if (valid) {
@@ -96,13 +96,13 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
     }
     __syncthreads();
     float2 *o = (r == A) ? B : A;
-    float2 *x = line_fft<false>(r, o, px, 1, t, tpr);
+    float2 *x = line_fft_sel<false, NC>(r, o, px, 1, t, tpr);
     if (valid)
       for (int i = t; i < n; i += tpr) a.dst[base + i] = x[i];
   } else if constexpr (MODE == ROW_DM_ITER) {
     const float beta = iter_beta(a);
-    float2 *rho = line_fft<true>(A, B, px, 1, t, tpr);
-    float2 *fr = line_fft<true>(Cb, D, px, 1, t, tpr);
+    float2 *rho = line_fft_sel<true, NC>(A, B, px, 1, t, tpr);
+    float2 *fr = line_fft_sel<true, NC>(Cb, D, px, 1, t, tpr);
     for (int i = t; i < n; i += tpr) {
       float2 g = make_float2(0.0f, 0.0f), f1 = g;
       if (valid) {
@@ -127,9 +127,9 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
     }
     __syncthreads();
     float2 *o1 = (rho == A) ? B : A;
-    float2 *x = line_fft<false>(rho, o1, px, 1, t, tpr);
+    float2 *x = line_fft_sel<false, NC>(rho, o1, px, 1, t, tpr);
     float2 *o2 = (fr == Cb) ? D : Cb;
-    float2 *xf = line_fft<false>(fr, o2, px, 1, t, tpr);
+    float2 *xf = line_fft_sel<false, NC>(fr, o2, px, 1, t, tpr);
     if (valid)
       for (int i = t; i < n; i += tpr) {
         a.dst[base + i] = x[i];
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
 }
 
 // ------------------------------------------------------------- column pass
-template <int MODE>
+template <int MODE, int NC>
 __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a, int ct, int tpc) {
   extern __shared__ float2 smem[];
   const int n = pl.n;
@@ -167,11 +167,11 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
 
   float2 *r;
   if constexpr (MODE == COL_FWD) {
-    r = line_fft<false>(A, B, pl, ct, t, tpc);
+    r = line_fft_sel<false, NC>(A, B, pl, ct, t, tpc);
   } else if constexpr (MODE == COL_INV || MODE == COL_INV_SQUARE_F32) {
-    r = line_fft<true>(A, B, pl, ct, t, tpc);
+    r = line_fft_sel<true, NC>(A, B, pl, ct, t, tpc);
   } else {
-    float2 *f = line_fft<false>(A, B, pl, ct, t, tpc);
+    float2 *f = line_fft_sel<false, NC>(A, B, pl, ct, t, tpc);
     if (valid) {
       for (int i = t; i < n; i += tpc) {
         const long long idx = lbase + i * a.estride;
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
     }
     __syncthreads();
     float2 *o2 = (f == A) ? B : A;
-    r = line_fft<true>(f, o2, pl, ct, t, tpc);
+    r = line_fft_sel<true, NC>(f, o2, pl, ct, t, tpc);
   }
   if (valid)
     for (int i = t; i < n; i += tpc) a.dst[lbase + i * a.estride] = r[(size_t)i * ct];
@@ -197,22 +197,49 @@ static int pow2_at_least(int v) {
   return p;
 }
 
-template <int MODE>
-static cudaError_t row_launch(const LinePlan &px, const PassArgs &a, cudaStream_t st) {
+// dynamic shared memory attribute, set once per kernel and size
+template <typename K>
+static cudaError_t smem_attr(K k, size_t smem, size_t &done) {
+  if (smem <= done) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) done = smem;
+  return e;
+}
+
+// lengths with a compile-time plan in the general kernels (the non-power-of-two
+// sizes of the mixed batches); others use the run-time plan
+#define SPB_CT_LENGTHS(X) X(192) X(384) X(1000)
+
+template <int MODE, int NC>
+static cudaError_t row_launch_n(const LinePlan &px, const PassArgs &a, cudaStream_t st) {
   const int n = px.n;
-  int tpr = pow2_at_least((n + 15) / 16);
+  int tpr = NC > 0 ? ct_max_butterflies(NC) : pow2_at_least((n + 15) / 16);
   if (tpr > 256) tpr = 256;
   if (tpr < 1) tpr = 1;
   const int rpb = 256 / tpr;
   const long long nrows = a.n / n;
   const int nbuf = (MODE == ROW_DM_ITER) ? 4 : 2;
   const size_t smem = (size_t)nbuf * rpb * n * sizeof(float2);
-  auto k = row_pass_kernel<MODE>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto k = row_pass_kernel<MODE, NC>;
+  static size_t done = 0;
+  cudaError_t e = smem_attr(k, smem, done);
   if (e != cudaSuccess) return e;
   const long long grid = (nrows + rpb - 1) / rpb;
   k<<<(unsigned)grid, rpb * tpr, smem, st>>>(px, a, tpr, rpb, nrows);
   return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t row_launch(const LinePlan &px, const PassArgs &a, cudaStream_t st) {
+  if (px.stw) {
+    switch (px.n) {
+#define SPB_CASE(n) \
+  case n: return row_launch_n<MODE, n>(px, a, st);
+      SPB_CT_LENGTHS(SPB_CASE)
+#undef SPB_CASE
+    }
+  }
+  return row_launch_n<MODE, 0>(px, a, st);
 }
 
 cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st) {
@@ -233,22 +260,37 @@ cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStre
   return cudaErrorInvalidValue;
 }
 
-template <int MODE>
-static cudaError_t col_launch(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+template <int MODE, int NC>
+static cudaError_t col_launch_n(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
   const int n = pl.n;
   int ct = 4096 / (n > 0 ? n : 1);
   if (ct > 16) ct = 16;
   if (ct < 1) ct = 1;
-  int tpc = pow2_at_least((n + 15) / 16);
+  int tpc = NC > 0 ? ct_max_butterflies(NC) : pow2_at_least((n + 15) / 16);
+  if (NC > 0 && tpc * ct > 1024) ct = 1024 / tpc > 0 ? 1024 / tpc : 1;  // keep one butterfly per thread
   if (tpc * ct > 1024) tpc = 1024 / ct;
   if (tpc * ct < 32) tpc = 32 / ct;
   const size_t smem = (size_t)2 * n * ct * sizeof(float2);
-  auto k = col_pass_kernel<MODE>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto k = col_pass_kernel<MODE, NC>;
+  static size_t done = 0;
+  cudaError_t e = smem_attr(k, smem, done);
   if (e != cudaSuccess) return e;
   dim3 grid((a.ncols + ct - 1) / ct, a.nouter);
   k<<<grid, ct * tpc, smem, st>>>(pl, a, ct, tpc);
   return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t col_launch(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+  if (pl.stw) {
+    switch (pl.n) {
+#define SPB_CASE(n) \
+  case n: return col_launch_n<MODE, n>(pl, a, st);
+      SPB_CT_LENGTHS(SPB_CASE)
+#undef SPB_CASE
+    }
+  }
+  return col_launch_n<MODE, 0>(pl, a, st);
 }
 
 cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArgs &a, cudaStream_t st) {
