@@ -209,15 +209,23 @@ static cudaError_t smem_attr(K k, size_t smem, size_t &done) {
 // lengths with a compile-time plan in the general kernels (the non-power-of-two
 // sizes of the mixed batches); others use the run-time plan
 #define SPB_CT_LENGTHS(X) X(192) X(384) X(1000)
+// the difference map's row passes have no register kernel: compile-time plans
+// for the power-of-two lengths too
+#define SPB_CT_LENGTHS_DM(X) X(64) X(128) X(256) X(512) X(1024) X(2048)
 
 template <int MODE, int NC>
 static cudaError_t row_launch_n(const LinePlan &px, const PassArgs &a, cudaStream_t st) {
   const int n = px.n;
-  int tpr = NC > 0 ? ct_max_butterflies(NC) : pow2_at_least((n + 15) / 16);
+  // compile-time plans: one butterfly per thread, at least two warps per row
+  int tpr = NC > 0 ? (ct_max_butterflies(NC) > 64 ? ct_max_butterflies(NC) : 64) : pow2_at_least((n + 15) / 16);
   if (tpr > 256) tpr = 256;
   if (tpr < 1) tpr = 1;
-  const int rpb = 256 / tpr;
   const long long nrows = a.n / n;
+  int rpb = 256 / tpr;
+  if (NC > 0) {  // no fewer blocks than two per SM when the rows allow it
+    const long long cap = nrows / 296;
+    if (cap < rpb) rpb = cap > 0 ? (int)cap : 1;
+  }
   const int nbuf = (MODE == ROW_DM_ITER) ? 4 : 2;
   const size_t smem = (size_t)nbuf * rpb * n * sizeof(float2);
   auto k = row_pass_kernel<MODE, NC>;
@@ -237,6 +245,14 @@ static cudaError_t row_launch(const LinePlan &px, const PassArgs &a, cudaStream_
   case n: return row_launch_n<MODE, n>(px, a, st);
       SPB_CT_LENGTHS(SPB_CASE)
 #undef SPB_CASE
+    }
+    if constexpr (MODE == ROW_DM_ITER || MODE == ROW_DM_F1_FWD) {
+      switch (px.n) {
+#define SPB_CASE(n) \
+  case n: return row_launch_n<MODE, n>(px, a, st);
+        SPB_CT_LENGTHS_DM(SPB_CASE)
+#undef SPB_CASE
+      }
     }
   }
   return row_launch_n<MODE, 0>(px, a, st);
