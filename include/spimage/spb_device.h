@@ -160,6 +160,22 @@ int spb_blur_host(int nx, int ny, int nz, const float *in, float radius, float *
  * src/support_update.c:392-400 with the area rule :143-144 or the threshold
  * rule :175-176): updates bit 0 of flags in place. */
 int spb_support_from_blur_host(long long n, const float *blur, int type, float value, int *flags);
+/* Phase-retrieval transfer function of n reconstructions (the reference's
+ * Python prtf, src/_spimage_prtf.py:17-106, over sp_image_superimpose and
+ * sp_image_phase_match, src/image_util.c:2974-3007,3160-3186), on the GPU.
+ * images: [n][N] complex (real space, as reconstructed), supports: [n][N].
+ * flags: bit 0 superimpose each image on the running sum (translation by
+ * cross-correlation of the moduli, then phase matching), bit 1 also try the
+ * enantiomorph.  Outputs (NULL skips): prtf[N] = |mean unit phasor of the
+ * images' spectra| (zero where a spectrum vanishes), in the FFT layout
+ * (the reference returns it fftshifted); super_image[N] complex = the sum of
+ * the aligned images; super_mask[N] = 1 where some non-empty support left
+ * the pixel out.  Translations and reflections are decided from the same
+ * correlation values as the reference (bit-exact FFTs); the phase matching
+ * sums in double and evaluates atan2/cos/sin on the GPU, so results agree
+ * with the reference to rounding, not bit for bit. */
+int spb_prtf_host(int nx, int ny, int nz, int n, const float *images, const int *supports, int flags, float *prtf,
+                  float *super_image, int *super_mask);
 /* No counterpart in the reference.  spb_support_from_blur_host without any
  * device allocation, for callers that must not allocate device memory: a
  * process whose HBM is reserved up front by another allocator (a framework's

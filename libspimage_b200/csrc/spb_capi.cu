@@ -1728,3 +1728,318 @@ extern "C" int spb_support_from_blur_noalloc(long long n, const float *blur, int
   CK(cudaStreamSynchronize(st));
   return 0;
 }
+
+// ------------------------------------------------------------------ PRTF
+// Phase-retrieval transfer function of n reconstructions, the reference's
+// Python prtf (src/_spimage_prtf.py:17-106) on the device: each image after
+// the first is superimposed on the running sum (sp_image_superimpose,
+// src/image_util.c:2974-3007: cross-correlation of the moduli, optionally the
+// convolution for the enantiomorph, argmax, reflection, wrap-around
+// translation), phase-matched to it (sp_image_phase_match weighted by |sum|^2,
+// src/image_util.c:3160-3186) and added; the PRTF is |mean of the unit
+// phasors of the images' spectra|, zero where any spectrum vanishes.
+namespace spb {
+__global__ void prtf_modulus_kernel(const float2 *in, float2 *out, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = make_float2(cabs_ref(in[i]), 0.0f);
+}
+// C = A * conj(B) (correlation) or A * B (convolution), sp_cmul's operation order
+__global__ void prtf_cmul_kernel(const float2 *A, const float2 *B, float2 *C, long long n, int conj) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 a = A[i];
+    float2 b = B[i];
+    if (conj) b.y = -b.y;
+    C[i] = make_float2(fsub(fmul(a.x, b.x), fmul(a.y, b.y)), fadd(fmul(a.x, b.y), fmul(b.x, a.y)));
+  }
+}
+// per block: largest |v*s| (sp_cscale then sp_cabs) and its first index
+__global__ void prtf_argmax_kernel(const float2 *v, long long n, float s, float *bval, long long *bidx) {
+  float best = -1.0f;
+  long long bi = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 x = v[i];
+    const float m = cabs_ref(make_float2(fmul(x.x, s), fmul(x.y, s)));
+    if (m > best) {
+      best = m;
+      bi = i;
+    }
+  }
+  __shared__ float sv[256];
+  __shared__ long long si[256];
+  sv[threadIdx.x] = best;
+  si[threadIdx.x] = bi;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      const float o = sv[threadIdx.x + w];
+      const long long oi = si[threadIdx.x + w];
+      if (o > sv[threadIdx.x] || (o == sv[threadIdx.x] && oi < si[threadIdx.x])) {
+        sv[threadIdx.x] = o;
+        si[threadIdx.x] = oi;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    bval[blockIdx.x] = sv[0];
+    bidx[blockIdx.x] = si[0];
+  }
+}
+// sp_image_reflect(SP_ORIGO) of the data (not the mask): both axes in 2-D; in
+// 3-D every plane mirrored through the centre except, for an odd depth, the
+// middle plane, which the reference's pairwise swap loop leaves unchanged
+__global__ void prtf_reflect_kernel(const float2 *in, float2 *out, int nx, int ny, int nz) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
+    if (nz > 1 && (nz & 1) && z == (nz - 1) / 2) {
+      out[i] = in[i];
+    } else {
+      const int zz = nz > 1 ? nz - 1 - z : z;
+      out[i] = in[((long long)zz * ny + (ny - 1 - y)) * nx + (nx - 1 - x)];
+    }
+  }
+}
+// wrap-around translation by (dx,dy,dz) of data and mask (sp_image_translate)
+__global__ void prtf_translate_kernel(const float2 *in, const int *min_, float2 *out, int *mout, int nx, int ny,
+                                      int nz, int dx, int dy, int dz) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
+    const int sx = ((x - dx) % nx + nx) % nx, sy = ((y - dy) % ny + ny) % ny, sz = ((z - dz) % nz + nz) % nz;
+    const long long s = ((long long)sz * ny + sy) * nx + sx;
+    out[i] = in[s];
+    mout[i] = min_[s];
+  }
+}
+// phase match: sum of |a|^2 exp(i(arg a - arg b)) (sums in double)
+__global__ void prtf_phase_sum_kernel(const float2 *a, const float2 *b, long long n, double *part) {
+  double sx = 0.0, sy = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 av = a[i], bv = b[i];
+    const float angle = (float)(atan2((double)av.y, (double)av.x) - atan2((double)bv.y, (double)bv.x));
+    const float mag = fadd(fmul(av.x, av.x), fmul(av.y, av.y));
+    sx += (double)(float)(cos((double)angle) * mag);
+    sy += (double)(float)(sin((double)angle) * mag);
+  }
+  __shared__ double s0[256], s1[256];
+  s0[threadIdx.x] = sx;
+  s1[threadIdx.x] = sy;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s0[threadIdx.x] += s0[threadIdx.x + w];
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s0[0];
+    part[2 * blockIdx.x + 1] = s1[0];
+  }
+}
+__global__ void prtf_phase_apply_kernel(float2 *b, long long n, float phi) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 v = b[i];
+    const float angle = (float)(atan2((double)v.y, (double)v.x) + (double)phi);
+    const float mag = cabs_ref(v);
+    b[i] = make_float2((float)(cos((double)angle) * mag), (float)(sin((double)angle) * mag));
+  }
+}
+// sum += img (sp_image_add); counts[mask == 0] += 1 when the support is not empty
+__global__ void prtf_add_kernel(float2 *sum, const float2 *img, const int *mask, float *counts, long long n,
+                                int count_mask) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 s = sum[i], v = img[i];
+    sum[i] = make_float2(fadd(s.x, v.x), fadd(s.y, v.y));
+    if (count_mask && mask[i] == 0) counts[i] = fadd(counts[i], 1.0f);
+  }
+}
+// unit phasors of a spectrum into the phasor sum; spectra that vanish count zeros
+__global__ void prtf_phasor_kernel(const float2 *F, float2 *sum, int *zeros, long long n, int init) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 f = F[i];
+    const float m = cabs_ref(f);
+    float2 u = make_float2(0.0f, 0.0f);
+    if (m > 0.0f) u = make_float2(__fdiv_rn(f.x, m), __fdiv_rn(f.y, m));
+    if (init) {
+      sum[i] = u;
+      zeros[i] = m > 0.0f ? 0 : 1;
+    } else {
+      const float2 s = sum[i];
+      sum[i] = make_float2(fadd(s.x, u.x), fadd(s.y, u.y));
+      if (!(m > 0.0f)) zeros[i] += 1;
+    }
+  }
+}
+__global__ void prtf_final_kernel(const float2 *sum, const int *zeros, const float *counts, float *prtf, int *smask,
+                                  long long n, float nimg) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 s = sum[i];
+    const float2 v = make_float2(__fdiv_rn(s.x, nimg), __fdiv_rn(s.y, nimg));
+    prtf[i] = zeros[i] > 0 ? 0.0f : cabs_ref(v);
+    smask[i] = counts[i] > 0.0f ? 1 : 0;
+  }
+}
+}  // namespace spb
+
+namespace {
+// forward / backward unnormalised transform of a whole context-sized buffer
+int prtf_fft(spb_ctx *c, const float2 *src, float2 *dst, int sign) {
+  PassArgs a = base_args(c);
+  if (sign < 0) {
+    a.src = src;
+    a.dst = dst;
+    if (row(c, ROW_FWD, a)) return -1;
+    return forward_rest(c, dst, dst);
+  }
+  if (backward_rest(c, src, c->T)) return -1;
+  a.src = c->T;
+  a.dst = dst;
+  return row(c, ROW_INV, a);
+}
+
+// largest |v * s| and its first index
+int prtf_argmax(spb_ctx *c, const float2 *v, float s, float *bval, long long *bidx, float *hval, long long *hidx,
+                float *best, long long *best_i) {
+  const int nblk = 296;
+  prtf_argmax_kernel<<<nblk, 256, 0, c->st>>>(v, c->n, s, bval, bidx);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(hval, bval, sizeof(float) * nblk, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(hidx, bidx, sizeof(long long) * nblk, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  float bv = -1.0f;
+  long long bi = 0;
+  for (int k = 0; k < nblk; k++)
+    if (hval[k] > bv || (hval[k] == bv && hidx[k] < bi)) {
+      bv = hval[k];
+      bi = hidx[k];
+    }
+  *best = bv;
+  *best_i = bi;
+  return 0;
+}
+}  // namespace
+
+extern "C" int spb_prtf_host(int nx, int ny, int nz, int n, const float *images, const int *supports, int flags,
+                             float *prtf, float *super_image, int *super_mask) {
+  if (n < 1) return fail("prtf of %d images", n);
+  spb_ctx *c = nullptr;
+  if (spb_ctx_create(&c, nx, ny, nz)) return -1;
+  const long long N = c->n;
+  const size_t nc = sizeof(float2) * (size_t)N;
+  const int nblk = 296;
+  float2 *scratch = nullptr;
+  int *mask = nullptr, *mask2 = nullptr, *zeros = nullptr, *smask = nullptr;
+  float *counts = nullptr, *bval = nullptr, *dprtf = nullptr;
+  long long *bidx = nullptr;
+  double *part = nullptr;
+  std::vector<float> hval(nblk);
+  std::vector<long long> hidx(nblk);
+  std::vector<double> hpart(2 * nblk);
+  int rc = 0;
+  auto alloc = [&](void **p, size_t bytes) {
+    if (!rc && cudaMalloc(p, bytes) != cudaSuccess) rc = fail("prtf: cudaMalloc(%zu) failed", bytes);
+  };
+  alloc((void **)&scratch, nc);
+  alloc((void **)&mask, sizeof(int) * N);
+  alloc((void **)&mask2, sizeof(int) * N);
+  alloc((void **)&zeros, sizeof(int) * N);
+  alloc((void **)&smask, sizeof(int) * N);
+  alloc((void **)&counts, sizeof(float) * N);
+  alloc((void **)&dprtf, sizeof(float) * N);
+  alloc((void **)&bval, sizeof(float) * nblk);
+  alloc((void **)&bidx, sizeof(long long) * nblk);
+  alloc((void **)&part, sizeof(double) * 2 * nblk);
+  float2 *avg = c->g[0], *img = c->g[1], *A = c->X, *B = c->Y, *C = c->T, *sum = c->gp;
+  const float inv_n = (float)(1.0 / (double)N);
+  const int translate = flags & 1, enantio = flags & 2;
+  // image 0: the running sum and the first unit phasors
+  if (!rc && cudaMemcpyAsync(avg, images, nc, cudaMemcpyHostToDevice, c->st) != cudaSuccess) rc = fail("prtf: upload");
+  if (!rc && cudaMemsetAsync(counts, 0, sizeof(float) * N, c->st) != cudaSuccess) rc = fail("prtf: memset");
+  if (!rc) rc = prtf_fft(c, avg, scratch, -1);
+  if (!rc) {
+    prtf_phasor_kernel<<<1184, 256, 0, c->st>>>(scratch, sum, zeros, N, 1);
+    if (cudaGetLastError() != cudaSuccess) rc = fail("prtf: phasor kernel");
+  }
+  for (int i = 1; i < n && !rc; i++) {
+    const float *hi = images + 2 * (size_t)N * i;
+    const int *hm = supports + (size_t)N * i;
+    long long msum = 0;
+    for (long long k = 0; k < N; k++) msum += hm[k];
+    if (cudaMemcpyAsync(img, hi, nc, cudaMemcpyHostToDevice, c->st) != cudaSuccess ||
+        cudaMemcpyAsync(mask, hm, sizeof(int) * N, cudaMemcpyHostToDevice, c->st) != cudaSuccess) {
+      rc = fail("prtf: upload");
+      break;
+    }
+    if (translate) {
+      // cross-correlation and (optionally) convolution of the moduli
+      prtf_modulus_kernel<<<1184, 256, 0, c->st>>>(avg, scratch, N);
+      if (prtf_fft(c, scratch, A, -1)) { rc = -1; break; }
+      prtf_modulus_kernel<<<1184, 256, 0, c->st>>>(img, scratch, N);
+      if (prtf_fft(c, scratch, B, -1)) { rc = -1; break; }
+      prtf_cmul_kernel<<<1184, 256, 0, c->st>>>(A, B, scratch, N, 1);
+      if (prtf_fft(c, scratch, C, 1)) { rc = -1; break; }
+      float m1, m2 = -1.0f;
+      long long i1, i2 = 0;
+      if (prtf_argmax(c, C, inv_n, bval, bidx, hval.data(), hidx.data(), &m1, &i1)) { rc = -1; break; }
+      long long x = i1 % nx, y = (i1 / nx) % ny, z = i1 / ((long long)nx * ny);
+      bool reflect = false;
+      if (enantio) {
+        prtf_cmul_kernel<<<1184, 256, 0, c->st>>>(A, B, scratch, N, 0);
+        if (prtf_fft(c, scratch, C, 1)) { rc = -1; break; }
+        if (prtf_argmax(c, C, inv_n, bval, bidx, hval.data(), hidx.data(), &m2, &i2)) { rc = -1; break; }
+        if (m2 > m1) {
+          reflect = true;
+          x = i2 % nx + 1;
+          y = (i2 / nx) % ny + 1;
+          z = i2 / ((long long)nx * ny) + 1;
+        }
+      }
+      if (reflect) {
+        prtf_reflect_kernel<<<1184, 256, 0, c->st>>>(img, scratch, nx, ny, nz);
+        if (cudaMemcpyAsync(img, scratch, nc, cudaMemcpyDeviceToDevice, c->st) != cudaSuccess) { rc = fail("prtf"); break; }
+      }
+      prtf_translate_kernel<<<1184, 256, 0, c->st>>>(img, mask, scratch, mask2, nx, ny, nz, (int)x, (int)y, (int)z);
+      if (cudaMemcpyAsync(img, scratch, nc, cudaMemcpyDeviceToDevice, c->st) != cudaSuccess ||
+          cudaMemcpyAsync(mask, mask2, sizeof(int) * N, cudaMemcpyDeviceToDevice, c->st) != cudaSuccess) {
+        rc = fail("prtf: translate");
+        break;
+      }
+      // phase match to the running sum
+      prtf_phase_sum_kernel<<<nblk, 256, 0, c->st>>>(avg, img, N, part);
+      if (cudaMemcpyAsync(hpart.data(), part, sizeof(double) * 2 * nblk, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+          cudaStreamSynchronize(c->st) != cudaSuccess) {
+        rc = fail("prtf: phase sum");
+        break;
+      }
+      double sx = 0.0, sy = 0.0;
+      for (int k = 0; k < nblk; k++) {
+        sx += hpart[2 * k];
+        sy += hpart[2 * k + 1];
+      }
+      const float phi = (float)atan2((double)(float)sy, (double)(float)sx);
+      prtf_phase_apply_kernel<<<1184, 256, 0, c->st>>>(img, N, phi);
+    }
+    prtf_add_kernel<<<1184, 256, 0, c->st>>>(avg, img, mask, counts, N, msum > 0);
+    if (prtf_fft(c, img, scratch, -1)) { rc = -1; break; }
+    prtf_phasor_kernel<<<1184, 256, 0, c->st>>>(scratch, sum, zeros, N, 0);
+    if (cudaGetLastError() != cudaSuccess) rc = fail("prtf: kernel launch failed");
+  }
+  if (!rc) {
+    prtf_final_kernel<<<1184, 256, 0, c->st>>>(sum, zeros, counts, dprtf, smask, N, (float)n);
+    if (cudaGetLastError() != cudaSuccess) rc = fail("prtf: kernel launch failed");
+  }
+  if (!rc && prtf && cudaMemcpyAsync(prtf, dprtf, sizeof(float) * N, cudaMemcpyDeviceToHost, c->st) != cudaSuccess)
+    rc = fail("prtf: download");
+  if (!rc && super_image && cudaMemcpyAsync(super_image, avg, nc, cudaMemcpyDeviceToHost, c->st) != cudaSuccess)
+    rc = fail("prtf: download");
+  if (!rc && super_mask && cudaMemcpyAsync(super_mask, smask, sizeof(int) * N, cudaMemcpyDeviceToHost, c->st) != cudaSuccess)
+    rc = fail("prtf: download");
+  if (!rc && cudaStreamSynchronize(c->st) != cudaSuccess) rc = fail("prtf: device error");
+  void *ptrs[] = {scratch, mask, mask2, zeros, smask, counts, dprtf, bval, bidx, part};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  spb_ctx_destroy(c);
+  return rc;
+}
