@@ -37,6 +37,14 @@ const char *spb_error_string(void);
 /* Number of usable CUDA devices (0 when there is none or the driver fails). */
 int spb_device_count(void);
 
+/* Self-check of the branch-free correctly rounded square root and quotient
+ * that the projection passes use (no counterpart in the reference): compares
+ * them bit for bit with the IEEE intrinsics on every float whose bit pattern
+ * lies in [lo, hi) inside the square-root domain, and on ndiv pseudo-random
+ * quotients drawn from seed; returns the mismatch counts (expected 0). */
+int spb_check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
+                        unsigned long long *bad_sqrt, unsigned long long *bad_div);
+
 /* Context for one nx*ny*nz problem on the current CUDA device; replaces the
  * device buffers the reference allocates in sp_phaser_set_amplitudes and
  * sp_phaser_init_model (src/phasing.c:322-330,706-721). */

@@ -46,6 +46,20 @@ static int fail(const char *fmt, ...) {
 
 extern "C" const char *spb_error_string(void) { return g_err; }
 
+extern "C" int spb_check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
+                                   unsigned long long *bad_sqrt, unsigned long long *bad_div) {
+  unsigned long long *d = nullptr, h[2] = {0, 0};
+  if (cudaMalloc(&d, sizeof h) != cudaSuccess) return fail("cudaMalloc failed");
+  cudaError_t e = cudaMemset(d, 0, sizeof h);
+  if (e == cudaSuccess) e = check_roundings(lo, hi, ndiv, seed, d);
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail("rounding self-check: %s", cudaGetErrorString(e));
+  if (bad_sqrt) *bad_sqrt = h[0];
+  if (bad_div) *bad_div = h[1];
+  return 0;
+}
+
 extern "C" int spb_device_count(void) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;

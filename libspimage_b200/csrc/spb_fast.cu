@@ -176,6 +176,44 @@ __device__ __forceinline__ float2 project_with(float2 G, float amp, bool measure
   return make_float2(amp, 0.0f);
 }
 
+// Projection of a thread's 16 points (line index i = t + T*q) with the
+// line's amplitudes and measured bits in shared memory.  When every measured
+// point's |G|^2 lies in the domain of the branch-free square root and
+// quotient (the common case) the 16 projections contain no branch, so the
+// compiler interleaves them; otherwise the thread projects all 16 with the
+// IEEE intrinsics.  Both give the bits of project_with.
+template <int T, bool FC>
+__device__ __forceinline__ void project16(float2 (&v)[16], const float *amp_l, const uint32_t *meas_l, int t,
+                                          size_t lbase, size_t qstride, const PassArgs &a) {
+  if (FC && (a.constraints & C_CENTROSYM))
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q].y = 0.0f;
+  bool fast = a.objective == 0 && !(a.constraints & C_MARGIN);
+  float s2[16];
+  unsigned mm = 0;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int i = t + T * q;
+    const unsigned meas = (meas_l[i >> 5] >> (i & 31)) & 1u;
+    mm |= meas << q;
+    s2[q] = fadd(fmul(v[q].y, v[q].y), fmul(v[q].x, v[q].x));
+    fast = fast && (!meas || sqrt_rn_nb_domain(s2[q]));
+  }
+  if (fast) {
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const float amp = amp_l[t + T * q];
+      const float m = div_rn_nb(amp, sqrt_rn_nb(s2[q]));
+      const float2 p = isfinite(m) ? make_float2(fmul(v[q].x, m), fmul(v[q].y, m)) : make_float2(amp, 0.0f);
+      if ((mm >> q) & 1u) v[q] = p;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+      v[q] = project_with(v[q], amp_l[t + T * q], (mm >> q) & 1u, lbase + q * qstride, a, false);
+  }
+}
+
 // words per line of the measured-bit bitmap (a multiple of 4 words)
 __host__ __device__ constexpr int proj_words(int n) { return ((n + 127) / 128) * 4; }
 template <int N, int C>
@@ -350,20 +388,15 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
   } else {
     reg::fft<N, false>(v, line, t, tw_s);
     if (valid) {
+      if constexpr (PREFETCH) {
+        project16<T, MODE == COL_PROJECT>(v, amp_s + c * SA, meas_s + c * SW, t, lbase, qstride, a);
+      } else {
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const size_t idx = lbase + q * qstride;
-        if constexpr (PREFETCH) {
-          const int i = t + T * q;
-          const float amp = amp_s[c * SA + i];
-          const bool meas = (meas_s[c * SW + (i >> 5)] >> (i & 31)) & 1u;
-          v[q] = project_with(v[q], amp, meas, idx, a, MODE == COL_PROJECT);
-        } else if constexpr (MODE == COL_PROJECT) {
-          v[q] = project(v[q], idx, a, true);
-        } else if constexpr (MODE == COL_PROJECT_NOFC) {
-          v[q] = project(v[q], idx, a, false);
-        } else {
-          v[q] = gauss_mult(v[q], idx, a);
+        for (int q = 0; q < 16; q++) {
+          const size_t idx = lbase + q * qstride;
+          if constexpr (MODE == COL_PROJECT) v[q] = project(v[q], idx, a, true);
+          else if constexpr (MODE == COL_PROJECT_NOFC) v[q] = project(v[q], idx, a, false);
+          else v[q] = gauss_mult(v[q], idx, a);
         }
       }
     }
@@ -373,6 +406,52 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
   if (valid)
 #pragma unroll
     for (int q = 0; q < 16; q++) a.dst[lbase + q * qstride] = v[q];
+}
+
+// ------------------------------------------- self-check of the roundings
+// Every float x in the square-root domain with bit pattern in [lo, hi), and
+// n pseudo-random quotients a/b with b in the quotient domain: counts the
+// results of the branch-free forms that differ in any bit from the IEEE
+// intrinsics'.
+__global__ void check_sqrt_kernel(unsigned lo, unsigned hi, unsigned long long *bad) {
+  unsigned long long nbad = 0;
+  for (unsigned long long u = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; u < hi;
+       u += (unsigned long long)gridDim.x * blockDim.x) {
+    const float x = __uint_as_float((unsigned)u);
+    if (!sqrt_rn_nb_domain(x)) continue;
+    nbad += __float_as_uint(sqrt_rn_nb(x)) != __float_as_uint(__fsqrt_rn(x));
+  }
+  if (nbad) atomicAdd(bad, nbad);
+}
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;  // splitmix64 finaliser
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void check_div_kernel(unsigned long long n, unsigned long long seed, unsigned long long *bad) {
+  unsigned long long nbad = 0;
+  for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long r = mix64(seed ^ mix64(k));
+    // a: any finite or non-finite pattern; b: exponent in [-63, 63), random sign-free significand
+    const float a = __uint_as_float((unsigned)r);
+    const unsigned eb = 64u + (unsigned)((r >> 32) % 126u);
+    const float b = __uint_as_float((eb << 23) | ((unsigned)(r >> 40) & 0x7FFFFFu));
+    const float q = div_rn_nb(a, b), ref = __fdiv_rn(a, b);
+    const bool both_nan = isnan(q) && isnan(ref);
+    nbad += !both_nan && __float_as_uint(q) != __float_as_uint(ref);
+  }
+  if (nbad) atomicAdd(bad, nbad);
+}
+
+cudaError_t check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
+                            unsigned long long *d_bad) {
+  check_sqrt_kernel<<<148 * 8, 256>>>(lo, hi, d_bad);
+  check_div_kernel<<<148 * 8, 256>>>(ndiv, seed, d_bad + 1);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- launch

@@ -104,6 +104,8 @@ struct SelectState {
 // line length or mode has none
 cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
+cudaError_t check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
+                            unsigned long long *d_bad);
 
 // host-side launchers (spb_kernels.cu): register kernels where available,
 // general kernels otherwise

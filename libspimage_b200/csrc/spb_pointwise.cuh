@@ -31,6 +31,55 @@ __device__ __forceinline__ float2 apply_constraints(float2 g, uint8_t f, int c) 
   return g;
 }
 
+// ---------------------------------------------------------------------------
+// Branch-free correctly rounded square root and quotient of floats.
+//
+// Method: evaluate the result in double precision to within one double ulp
+// (relative error < 2^-52), then round once to float.  A float square root or
+// quotient is never a float midpoint, and its distance from the nearest
+// midpoint is at least 2^-51 (square root) or 2^-49 (quotient) relative: the
+// midpoint M*2^e has an odd 25-bit M, so x - m^2 (resp. a - m*b) is a nonzero
+// multiple of the finer of the two grids.  A faithful double therefore lies on
+// the same side of every midpoint as the exact value and rounds to the
+// correctly rounded float (the double-rounding bound of S. Figueroa, "When is
+// double rounding innocuous?", SIGNUM Newsletter 30(3), 1995: p' >= 2p + 2).
+// The seeds are the hardware approximations of PTX rsqrt.approx.f32 (relative
+// error <= 2^-22.9) and rcp.approx.f32 (<= 1 ulp), refined by one Taylor step
+// in double:
+//   sqrt(x) = g (1 - r)^(-1/2) = g (1 + r/2 + 3r^2/8 + O(r^3)),  g = x t,  r = 1 - x t^2
+//   1/b     = t (1 - e)^(-1)   = t (1 + e + e^2 + O(e^3)),        e = 1 - b t
+// with |r|, |e| < 2^-21, so the truncation (< 2^-62) and the roundings of the
+// small terms are far below the last rounding.  Domain: x in [2^-126, 2^126]
+// (normal, with a normal reciprocal square root); b in [2^-63, 2^63]; a any
+// float (an infinite or NaN a propagates; an overflowing quotient rounds to
+// infinity as the IEEE quotient does).  Outside the domain the callers use
+// the IEEE intrinsics.
+__device__ __forceinline__ float rsqrt_seed(float x) {
+  float t;
+  asm("rsqrt.approx.f32 %0, %1;" : "=f"(t) : "f"(x));
+  return t;
+}
+__device__ __forceinline__ float rcp_seed(float x) {
+  float t;
+  asm("rcp.approx.f32 %0, %1;" : "=f"(t) : "f"(x));
+  return t;
+}
+__device__ __forceinline__ bool sqrt_rn_nb_domain(float x) { return x >= 0x1p-126f && x <= 0x1p126f; }
+__device__ __forceinline__ float sqrt_rn_nb(float x) {
+  const double X = (double)x, T = (double)rsqrt_seed(x);
+  const double G = X * T;                 // exact: 24 x 24 bits
+  const double R = fma(-G, T, 1.0);       // 1 - x t^2
+  const double H = R * fma(0.375, R, 0.5);
+  return __double2float_rn(fma(G, H, G));
+}
+// a / b for b in [2^-63, 2^63]
+__device__ __forceinline__ float div_rn_nb(float a, float b) {
+  const double B = (double)b, T = (double)rcp_seed(b);
+  const double E = fma(-B, T, 1.0);       // 1 - b t, exact (Sterbenz)
+  const double Y = fma(T, fma(E, E, E), T);
+  return __double2float_rn((double)a * Y);
+}
+
 // Fourier-space projection at pixel idx (src/phasing.c:1061-1109)
 __device__ __forceinline__ float2 project(float2 G, long long idx, const PassArgs &a, bool fourier_constraints) {
   const uint8_t f = a.flags[idx];
