@@ -72,8 +72,12 @@ const char *spb_kernel_name(int kind);
  * choice, 256 threads per block); SPB_TUNE_NO_PDL = 1 launches the pass
  * kernels without programmatic dependent launch (on by default: a pass
  * kernel stages its twiddles and the previous iterate while its predecessor
- * finishes).  Setting a knob drops the context's captured graphs. */
-enum { SPB_TUNE_ROW_LINES = 0, SPB_TUNE_NO_PDL = 1, SPB_TUNE_KNOBS = 4 };
+ * finishes); SPB_TUNE_ROW_G0 = where the iteration's row pass stages the
+ * previous iterate: 1 at the start (overlapping the inverse transform), 2
+ * between the two transforms (less shared memory, more blocks per SM), 0
+ * the built-in choice (2 when the grid exceeds what fits on the device at
+ * once with 1).  Setting a knob drops the context's captured graphs. */
+enum { SPB_TUNE_ROW_LINES = 0, SPB_TUNE_NO_PDL = 1, SPB_TUNE_ROW_G0 = 2, SPB_TUNE_KNOBS = 4 };
 int spb_ctx_set_tuning(spb_ctx *ctx, int knob, int value);
 int spb_ctx_get_tuning(spb_ctx *ctx, int knob);
 /* Autotuner (no reference counterpart): times `calls` calls of `iterations`

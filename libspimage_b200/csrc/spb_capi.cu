@@ -250,6 +250,7 @@ PassArgs base_args(const spb_ctx *c) {
   a.meas_bits = c->meas_bits;
   a.meas_words = c->meas_words;
   a.row_lpb = c->tune[SPB_TUNE_ROW_LINES];
+  a.row_g0 = c->tune[SPB_TUNE_ROW_G0];
   a.pdl = c->tune[SPB_TUNE_NO_PDL] ? 0 : 1;
   a.inv_n = (float)(1.0 / (double)c->n);
   a.nx_f = (float)c->nx;
@@ -1384,7 +1385,17 @@ struct TuneKey {
   }
 };
 std::mutex g_tune_mu;
-std::map<TuneKey, std::pair<int, int>> g_tune_cache;  // -> (row lines, no-pdl)
+struct TuneChoice {
+  int lines, nopdl, g0;
+};
+std::map<TuneKey, TuneChoice> g_tune_cache;
+
+int apply_choice(spb_ctx *c, const TuneChoice &t) {
+  if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, t.lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, t.nopdl) ||
+      spb_ctx_set_tuning(c, SPB_TUNE_ROW_G0, t.g0))
+    return -1;
+  return 0;
+}
 }  // namespace
 
 extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterations, int calls, int force,
@@ -1397,8 +1408,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
       if (best_ms) *best_ms = -1.0;
-      if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, it->second.first)) return -1;
-      return spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, it->second.second);
+      return apply_choice(c, it->second);
     }
   }
   // save the state the timed iterations overwrite
@@ -1413,7 +1423,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   }
   const int cur0 = c->cur, xv0 = c->x_valid, xfv0 = c->xf_valid;
   const float xfg0 = c->xf_gamma1;
-  const int knob0[2] = {c->tune[SPB_TUNE_ROW_LINES], c->tune[SPB_TUNE_NO_PDL]};
+  const TuneChoice knob0{c->tune[SPB_TUNE_ROW_LINES], c->tune[SPB_TUNE_NO_PDL], c->tune[SPB_TUNE_ROW_G0]};
   int rc = 0;
   const float2 *bufs[4] = {c->g[0], c->g[1], c->gp, c->X};
   for (int k = 0; k < 4 && !rc; k++)
@@ -1428,11 +1438,13 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   const int T = c->nx >= 16 ? c->nx / 16 : 1;
   const int lpb_max = 256 / T > 0 ? 256 / T : 1;
   double best = 1e30;
-  int best_lines = 0, best_nopdl = 0;
-  for (int nopdl = 0; nopdl < 2 && !rc; nopdl++) {
-    for (int lines = 0; lines <= lpb_max && !rc; lines = lines ? lines * 2 : 1) {
-      if (lines == lpb_max) continue;  // the same as the built-in choice (0)
-      if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, nopdl)) {
+  TuneChoice bestc{0, 0, 0};
+  for (int cand = 0; cand < 2 * 2 * 16 && !rc; cand++) {
+    const int nopdl = cand & 1, g0 = 1 + ((cand >> 1) & 1), li = cand >> 2;
+    const int lines = li ? 1 << (li - 1) : 0;
+    if (lines >= lpb_max) continue;  // lpb_max is the built-in choice (0)
+    {
+      if (apply_choice(c, TuneChoice{lines, nopdl, g0})) {
         rc = -1;
         break;
       }
@@ -1447,8 +1459,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
         rc = fail("autotune: timing failed");
       if (!rc && ms < best) {
         best = ms;
-        best_lines = lines;
-        best_nopdl = nopdl;
+        bestc = TuneChoice{lines, nopdl, g0};
       }
     }
   }
@@ -1467,15 +1478,13 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   (void)xfv0;
   (void)xfg0;
   if (rc) {
-    spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, knob0[0]);
-    spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, knob0[1]);
+    apply_choice(c, knob0);
     return -1;
   }
-  if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, best_lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, best_nopdl))
-    return -1;
+  if (apply_choice(c, bestc)) return -1;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[key] = std::make_pair(best_lines, best_nopdl);
+    g_tune_cache[key] = bestc;
   }
   if (best_ms) *best_ms = best / (double)((size_t)calls * iterations);
   return 0;

@@ -227,8 +227,12 @@ __host__ __device__ constexpr int bits_stride() {
 
 // ------------------------------------------------------------ row kernels
 // Shared memory: [twiddles N][LPB exchange lines of N+N/16]
-//                (ROW_ITER) [LPB rows of g0][LPB rows of flags]
-template <int N, int MODE>
+//                (ROW_ITER) [LPB rows of g0, unless G0LATE][LPB rows of flags]
+// ROW_ITER copies g0 either at the start, to overlap its load with the
+// inverse transform (latency-bound grids), or with G0LATE into each row's
+// exchange line between the two transforms (the line is free then): less
+// shared memory per block, so more blocks share an SM (throughput-bound grids).
+template <int N, int MODE, bool G0LATE>
 __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 *__restrict__ stw, int nrows) {
   constexpr int T = N / 16;
   constexpr int S = N + N / 16;
@@ -244,13 +248,15 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
   stage_twiddles<N>(tw_s, stw);
   // g0 rows start on a 16-byte boundary (an even float2 offset) for the 16-byte copies
   float2 *g0_s = sm + ((N + lpb * S + 1) & ~1);
-  uint8_t *fl_s = reinterpret_cast<uint8_t *>(g0_s + lpb * N);
+  uint8_t *fl_s = reinterpret_cast<uint8_t *>(g0_s + (G0LATE ? 0 : lpb * N));
+  const int vrows = min(lpb, nrows - row0);
   if constexpr (MODE == ROW_ITER) {
-    // g0 and flags of this block's rows: contiguous, copied in 16-byte chunks
-    const int vrows = min(lpb, nrows - row0);
-    const float2 *g0src = a.g0 + (size_t)row0 * N;
-    const int nchunk = vrows * N / 2;
-    for (int c = threadIdx.x; c < nchunk; c += blockDim.x) cp_async16(g0_s + 2 * c, g0src + 2 * c);
+    // g0 (unless G0LATE) and flags of this block's rows: contiguous, copied in 16-byte chunks
+    if constexpr (!G0LATE) {
+      const float2 *g0src = a.g0 + (size_t)row0 * N;
+      const int nchunk = vrows * N / 2;
+      for (int c = threadIdx.x; c < nchunk; c += blockDim.x) cp_async16(g0_s + 2 * c, g0src + 2 * c);
+    }
     const uint8_t *fsrc = a.flags + (size_t)row0 * N;
     const int fchunk = vrows * N / 16;
     for (int c = threadIdx.x; c < fchunk; c += blockDim.x) cp_async16(fl_s + 16 * c, fsrc + 16 * c);
@@ -293,7 +299,26 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
     const float beta = iter_beta(a);
     const float one_m2b = fsub(1.0f, fmul(2.0f, beta));  // 1 - 2*beta in float, as the reference
     reg::fft<N, true>(v, line, t, tw_s);
-    const float2 *g0r = g0_s + lr * N + t;
+    // G0LATE: g0 of the block's rows into their exchange lines; the
+    // transform's last stage uses registers only, and a barrier followed its
+    // last exchange
+    if constexpr (G0LATE) {
+      const float2 *g0src = a.g0 + (size_t)row0 * N;
+      if constexpr (S % 2 == 0) {
+        for (int c = threadIdx.x; c < vrows * (N / 2); c += blockDim.x) {
+          const int r = c / (N / 2), j = c % (N / 2);
+          cp_async16(sm + N + r * S + 2 * j, g0src + (size_t)r * N + 2 * j);
+        }
+      } else {
+        for (int c = threadIdx.x; c < vrows * N; c += blockDim.x) {
+          const int r = c / N, j = c % N;
+          cp_async8(sm + N + r * S + j, g0src + (size_t)r * N + j);
+        }
+      }
+      cp_async_wait_all();
+      __syncthreads();
+    }
+    const float2 *g0r = G0LATE ? line + t : g0_s + lr * N + t;
     const uint8_t *flr = fl_s + lr * N + t;
     float2 *gp = a.gp;
 #pragma unroll
@@ -318,6 +343,7 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
       }
       v[q] = g;
     }
+    if constexpr (G0LATE) __syncthreads();  // every g0 read done before the forward transform writes the lines
     reg::fft<N, false>(v, line, t, tw_s);
     pdl_release();
     if (valid)
@@ -463,23 +489,55 @@ static cudaError_t set_smem(K k, size_t smem, bool &done) {
   return e;
 }
 
+// dynamic shared memory limit of kernel K raised to at least smem (once per size)
+template <auto K>
+static cudaError_t ensure_smem(size_t smem) {
+  static size_t have = 0;
+  if (smem <= have) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) have = smem;
+  return e;
+}
+
 template <int N, int MODE>
 static cudaError_t row_fast_launch(const LinePlan &px, const PassArgs &a, cudaStream_t st) {
   constexpr int T = N / 16;
   constexpr int LPB_MAX = (256 / T) > 0 ? (256 / T) : 1;  // 256 threads per block at most
   const int LPB = (a.row_lpb > 0 && a.row_lpb < LPB_MAX) ? a.row_lpb : LPB_MAX;
   const long long nrows = a.n / N;
-  size_t smem = (size_t)((N + LPB * (N + N / 16) + 1) & ~1) * sizeof(float2);
-  if (MODE == ROW_ITER) smem += (size_t)LPB * N * (sizeof(float2) + 1);
-  auto k = row_fast_kernel<N, MODE>;
-  static bool done = false;
-  static size_t done_smem = 0;
-  if (smem > done_smem) done = false;
-  cudaError_t e = set_smem(k, smem, done);
-  if (e != cudaSuccess) return e;
-  if (smem > done_smem) done_smem = smem;
   const long long grid = (nrows + LPB - 1) / LPB;
-  return launch_maybe_pdl(k, dim3((unsigned)grid), dim3(LPB * T), smem, st, a.pdl != 0, a, px.stw, (int)nrows);
+  const size_t smem0 = (size_t)((N + LPB * (N + N / 16) + 1) & ~1) * sizeof(float2);
+  if constexpr (MODE == ROW_ITER) {
+    // g0 staging: SPB_TUNE_ROW_G0 1 = at the start, 2 = between the
+    // transforms; 0 = between the transforms when the grid is larger than the
+    // blocks that fit on the device at once with the larger staging
+    const size_t smem_early = smem0 + (size_t)LPB * N * (sizeof(float2) + 1), smem_late = smem0 + (size_t)LPB * N;
+    bool late = a.row_g0 == 2;
+    if (a.row_g0 == 0) {
+      static int nsm = 0;
+      if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) return cudaGetLastError();
+      int per_sm = 0;
+      cudaError_t e = ensure_smem<row_fast_kernel<N, MODE, false>>(smem_early);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, row_fast_kernel<N, MODE, false>, LPB * T, smem_early);
+      if (e != cudaSuccess) return e;
+      late = grid > (long long)per_sm * nsm;
+    }
+    if (late) {
+      cudaError_t e = ensure_smem<row_fast_kernel<N, MODE, true>>(smem_late);
+      if (e != cudaSuccess) return e;
+      return launch_maybe_pdl(row_fast_kernel<N, MODE, true>, dim3((unsigned)grid), dim3(LPB * T), smem_late, st,
+                              a.pdl != 0, a, px.stw, (int)nrows);
+    }
+    cudaError_t e = ensure_smem<row_fast_kernel<N, MODE, false>>(smem_early);
+    if (e != cudaSuccess) return e;
+    return launch_maybe_pdl(row_fast_kernel<N, MODE, false>, dim3((unsigned)grid), dim3(LPB * T), smem_early, st,
+                            a.pdl != 0, a, px.stw, (int)nrows);
+  }
+  cudaError_t e = ensure_smem<row_fast_kernel<N, MODE, false>>(smem0);
+  if (e != cudaSuccess) return e;
+  return launch_maybe_pdl(row_fast_kernel<N, MODE, false>, dim3((unsigned)grid), dim3(LPB * T), smem0, st,
+                          a.pdl != 0, a, px.stw, (int)nrows);
 }
 
 template <int N>

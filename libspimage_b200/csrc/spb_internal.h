@@ -70,6 +70,7 @@ struct PassArgs {
   int meas_words;
   // launch shape: lines per block of the row pass (0: the built-in choice)
   int row_lpb;
+  int row_g0;  // g0 staging of the register row pass: 0 auto, 1 at the start, 2 between the transforms
   // 1: launch the register pass kernels with programmatic dependent launch
   int pdl;
   // scalars

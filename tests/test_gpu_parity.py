@@ -202,17 +202,17 @@ def test_close_centre_batched_starts(lib):
                                            ((16, 16, 16), RAAR, [(AREA, 10, 2.0, 0.1)])])
 def test_autotune_and_launch_shapes_leave_results_unchanged(lib, oracle_mod, shape, alg, sup):
     """the autotuner restores the reconstruction it times on, and every
-    launch shape (row lines per block, dependent launch on/off) computes the
-    same bits"""
+    launch shape (row lines per block, dependent launch on/off, where the
+    row pass stages the previous iterate) computes the same bits"""
     ref = setup(oracle_mod.Restatement(shape), shape, alg, sup)
     tuned = setup(lib.Phaser(shape), shape, alg, sup)
     assert tuned.iterate(7) == 0 and ref.iterate(7) == 0
     choice = tuned.autotune()
-    assert choice["row_lines"] >= 0 and choice["no_pdl"] in (0, 1)
+    assert choice["row_lines"] >= 0 and choice["no_pdl"] in (0, 1) and choice["row_g0"] in (1, 2)
     assert tuned.autotune() == choice  # cached
     assert tuned.iterate(45) == 0 and ref.iterate(45) == 0
     _compare(tuned, ref)
-    for knob, value in ((0, 1), (0, 2), (1, 1)):
+    for knob, value in ((0, 1), (0, 2), (1, 1), (2, 1), (2, 2)):
         other = setup(lib.Phaser(shape), shape, alg, sup)
         other.set_tuning(knob, value)
         assert other.iterate(52) == 0
