@@ -197,6 +197,7 @@ struct spb_ctx {
   int cur = 0;
   float2 *X = nullptr, *Y = nullptr, *Xf = nullptr, *Yf = nullptr, *gp = nullptr, *T = nullptr;
   float *absb = nullptr;
+  float *gtab = nullptr;  // blur factor table, (nx/2+1)(ny/2+1)(nz/2+1)
   // line-major operands of the projection pass (lines along the last axis)
   float *amp_line = nullptr;
   uint32_t *meas_bits = nullptr;
@@ -262,6 +263,7 @@ PassArgs base_args(const spb_ctx *c) {
 // 2 = z lines (one set per start), 0 = lines of length 1 over every pixel
 // (pointwise pass for 1-D problems).
 void col_geometry(const spb_ctx *c, int axis, PassArgs &a, const LinePlan **pl) {
+  a.line_axis = axis;
   if (axis == 1) {
     a.estride = c->nx;
     a.ostride = (long long)c->nx * c->ny;
@@ -439,6 +441,8 @@ int check_dims(int nx, int ny, int nz, int nb) {
   return 0;
 }
 
+long long gauss_table_len(int nx, int ny, int nz) { return (long long)(nx / 2 + 1) * (ny / 2 + 1) * (nz / 2 + 1); }
+
 int check_start(const spb_ctx *c, int start) {
   if (start < 0 || start >= c->nb) return fail("start %d out of range [0, %d)", start, c->nb);
   return 0;
@@ -481,6 +485,7 @@ extern "C" int spb_ctx_create_batch(spb_ctx **out, int nx, int ny, int nz, int n
   alloc((void **)&c->gp, nc);
   alloc((void **)&c->T, nc);
   alloc((void **)&c->absb, nf);
+  alloc((void **)&c->gtab, sizeof(float) * (size_t)gauss_table_len(nx, ny, nz));
   alloc((void **)&c->sel, sizeof(SelectState) * (size_t)nb);
   alloc((void **)&c->red, sizeof(double) * (size_t)reduce_scratch_doubles(nb));
   alloc((void **)&c->seeds, sizeof(unsigned long long) * (size_t)nb);
@@ -570,6 +575,7 @@ extern "C" long long spb_ctx_footprint(int nx, int ny, int nz, int nb, int dm) {
   b += ntot;                                    // flags
   b += 6 * 8 * ntot;                            // g[2], X, Y, gp, T
   b += 4 * ntot;                                // absb
+  b += 4 * gauss_table_len(nx, ny, nz);         // gtab
   b += (long long)sizeof(SelectState) * nb;     // sel
   b += 8LL * reduce_scratch_doubles(nb);        // red
   b += 8LL * nb + 4 + 4LL * kBetaCap;           // seeds, beta_base, beta table
@@ -583,7 +589,7 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
-                  c->gp, c->T, c->absb, c->sel, c->red, c->ax.tw, c->ay.tw, c->az.tw,
+                  c->gp, c->T, c->absb, c->gtab, c->sel, c->red, c->ax.tw, c->ay.tw, c->az.tw,
                   c->amp_line, c->meas_bits, c->beta_dev, c->beta_base, c->seeds, c->beta_zero, c->spar};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1152,6 +1158,15 @@ extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float 
   return 0;
 }
 
+// the blur factor table of a's radius; a then looks factors up in it
+static int gauss_table(spb_ctx *c, PassArgs &a) {
+  a.blur_tab = nullptr;
+  CK(launch_gauss_table(a, c->gtab, c->st));
+  c->launches++;
+  a.blur_tab = c->gtab;
+  return 0;
+}
+
 // blur |g1| of every start (or |img| when img != nullptr) into c->absb
 static int blur_abs(spb_ctx *c, const float2 *img, float radius, const double *r2_dev = nullptr) {
   PassArgs a = base_args(c);
@@ -1161,6 +1176,7 @@ static int blur_abs(spb_ctx *c, const float2 *img, float radius, const double *r
   a.blur_c0 = -2. * pow(3.14159265358979323846, 2);
   a.blur_r2 = pow((double)radius, 2);
   a.blur_r2_dev = r2_dev;
+  if (gauss_table(c, a)) return -1;
   if (middle(c, COL_BLUR, c->T, c->T, a)) return -1;
   a.src = c->T;
   a.absout = c->absb;
@@ -1598,6 +1614,7 @@ extern "C" int spb_blur_host(int nx, int ny, int nz, const float *in, float radi
     if (row(c, ROW_FWD, a)) rc = -1;
     a.blur_c0 = -2. * pow(3.14159265358979323846, 2);
     a.blur_r2 = pow((double)radius, 2);
+    if (!rc && gauss_table(c, a)) rc = -1;
     if (!rc && middle(c, COL_BLUR, c->T, c->T, a)) rc = -1;
     a.src = c->T;
     a.dst = c->Y;

@@ -176,6 +176,51 @@ __device__ __forceinline__ float2 project_with(float2 G, float amp, bool measure
   return make_float2(amp, 0.0f);
 }
 
+// |v[q]| of 16 values as cabs_ref computes them: without a branch per value
+// when every |v|^2 is zero or in the domain of the branch-free square root,
+// else with the IEEE intrinsic for all 16 (the same bits either way)
+__device__ __forceinline__ void cabs16(const float2 (&v)[16], float (&r)[16]) {
+  bool fast = true;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    r[q] = fadd(fmul(v[q].y, v[q].y), fmul(v[q].x, v[q].x));
+    fast = fast && (r[q] == 0.0f || sqrt_rn_nb_domain(r[q]));
+  }
+  if (fast) {
+#pragma unroll
+    for (int q = 0; q < 16; q++) r[q] = r[q] == 0.0f ? r[q] : sqrt_rn_nb(r[q]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 16; q++) r[q] = __fsqrt_rn(r[q]);
+  }
+}
+
+// Blur factor of a thread's 16 points of a column line (line index t + T*q),
+// from the line's coordinates instead of per-point index arithmetic: the
+// same factors as gauss_mult.
+template <int T>
+__device__ __forceinline__ void blur16(float2 (&v)[16], int col, long long o, int t, const PassArgs &a) {
+  int x, y, z;  // coordinates of point q = 0; the line runs along y (axis 1) or z (axis 2)
+  if (a.line_axis == 2) {
+    x = col % a.nx;
+    y = col / a.nx;
+    z = t;
+  } else {
+    x = col;
+    y = t;
+    z = (int)(o % a.nz);
+  }
+  const int hx = a.nx / 2 + 1, hy = a.ny / 2 + 1;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int yy = a.line_axis == 2 ? y : y + T * q, zz = a.line_axis == 2 ? z + T * q : z;
+    const int dx = min(a.nx - x, x), dy = min(a.ny - yy, yy), dz = min(a.nz - zz, zz);
+    const float m = a.blur_tab ? a.blur_tab[((long long)dz * hy + dy) * hx + dx]
+                               : gauss_factor((float)dx, (float)dy, (float)dz, a);
+    v[q] = scale_cmul_dev(v[q], m);
+  }
+}
+
 // Projection of a thread's 16 points (line index i = t + T*q) with the
 // line's amplitudes and measured bits in shared memory.  When every measured
 // point's |G|^2 lies in the domain of the branch-free square root and
@@ -268,14 +313,19 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
     float2 x = make_float2(0.0f, 0.0f);
     if (valid) {
       const size_t idx = base + T * q;
-      if constexpr (MODE == ROW_FWD_DEPHASE) x = make_float2(cabs_ref(a.src[idx]), 0.0f);
-      else if constexpr (MODE == ROW_FWD_F32) x = make_float2(a.f32src[idx], 0.0f);
+      if constexpr (MODE == ROW_FWD_F32) x = make_float2(a.f32src[idx], 0.0f);
       else if constexpr (MODE == ROW_FWD_SQUARE_F32) {
         const float s = a.f32src[idx];
         x = make_float2(fmul(s, s), 0.0f);
       } else x = a.src[idx];
     }
     v[q] = x;
+  }
+  if constexpr (MODE == ROW_FWD_DEPHASE) {
+    float r[16];
+    cabs16(v, r);
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = make_float2(r[q], 0.0f);
   }
   cp_async_wait_all();
   __syncthreads();
@@ -287,13 +337,15 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
       for (int q = 0; q < 16; q++) a.dst[base + T * q] = v[q];
   } else if constexpr (MODE == ROW_INV || MODE == ROW_INV_SCALE || MODE == ROW_INV_ABS) {
     reg::fft<N, true>(v, line, t, tw_s);
+    float r[16];
+    if constexpr (MODE == ROW_INV_ABS) cabs16(v, r);
     pdl_release();
     if (valid)
 #pragma unroll
       for (int q = 0; q < 16; q++) {
         if constexpr (MODE == ROW_INV) a.dst[base + T * q] = v[q];
         else if constexpr (MODE == ROW_INV_SCALE) a.dst[base + T * q] = scale_cmul_dev(v[q], a.inv_n);
-        else a.absout[base + T * q] = cabs_ref(v[q]);
+        else a.absout[base + T * q] = r[q];
       }
   } else if constexpr (MODE == ROW_ITER) {
     const float beta = iter_beta(a);
@@ -422,8 +474,8 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
           const size_t idx = lbase + q * qstride;
           if constexpr (MODE == COL_PROJECT) v[q] = project(v[q], idx, a, true);
           else if constexpr (MODE == COL_PROJECT_NOFC) v[q] = project(v[q], idx, a, false);
-          else v[q] = gauss_mult(v[q], idx, a);
         }
+        if constexpr (MODE == COL_BLUR) blur16<T>(v, col, a.outer0 + blockIdx.y, t, a);
       }
     }
     reg::fft<N, true>(v, line, t, tw_s);

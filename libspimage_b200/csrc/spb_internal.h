@@ -49,6 +49,7 @@ struct PassArgs {
   long long ostride, estride;
   int ncols, nouter;
   long long outer0;  // first outer line of this launch (grids are split at 65535)
+  int line_axis;     // axis the column lines run along (1: y, outer = start*nz + z, column = x; 2: z, column = y*nx + x)
   // buffers
   const float2 *src;
   const float2 *src2;  // second input line (DM: Yf)
@@ -88,6 +89,7 @@ struct PassArgs {
   double blur_c0;   // -2*pow(pi,2) (host glibc)
   double blur_r2;   // pow(radius,2)
   const double *blur_r2_dev;  // when set, pow(radius,2) is read here (captured support updates)
+  const float *blur_tab;      // when set, the blur factor of distances (dx, dy, dz): [dz][dy][dx], n/2+1 each
   float nx_f;       // (float)nx
   float n_f;        // (float)N
 };
@@ -105,6 +107,7 @@ struct SelectState {
 // line length or mode has none
 cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_gauss_table(const PassArgs &a, float *tab, cudaStream_t st);
 cudaError_t check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
                             unsigned long long *d_bad);
 

@@ -324,6 +324,28 @@ cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArg
   return cudaErrorInvalidValue;
 }
 
+// --------------------------------------------------------- blur factor table
+// The Gaussian factor of every distance triple (dx, dy, dz) from the zero
+// frequency, dx in [0, nx/2] etc.: the blur's column pass looks the factor
+// up instead of evaluating it per pixel, and every start of a batch shares
+// the table.  Same function, same floats.
+__global__ void gauss_table_kernel(PassArgs a, float *__restrict__ tab) {
+  const int hx = a.nx / 2 + 1, hy = a.ny / 2 + 1;
+  const long long total = (long long)hx * hy * (a.nz / 2 + 1);
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int dx = (int)(t % hx), dy = (int)((t / hx) % hy), dz = (int)(t / ((long long)hx * hy));
+    tab[t] = gauss_factor((float)dx, (float)dy, (float)dz, a);
+  }
+}
+
+cudaError_t launch_gauss_table(const PassArgs &a, float *tab, cudaStream_t st) {
+  const long long total = (long long)(a.nx / 2 + 1) * (a.ny / 2 + 1) * (a.nz / 2 + 1);
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  gauss_table_kernel<<<(unsigned)blocks, 256, 0, st>>>(a, tab);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------- support selection kernels
 // Exact k-th largest value per start by most-significant-digit radix select
 // over the float bit patterns (non-negative floats order like their bits):
@@ -335,6 +357,9 @@ cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArg
 // starts.
 #define SEL_BITS 8
 #define SEL_BINS 256
+// Each thread loads SEL_UNROLL keys (independent loads in flight) before it
+// bins them; a warp skips the match when none of its keys carries the prefix.
+#define SEL_UNROLL 8
 __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restrict__ v, long long n, SelectState *s,
                                                           int shift) {
   __shared__ unsigned int h[8][SEL_BINS];
@@ -347,16 +372,23 @@ __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restric
   const unsigned int prefix = s->prefix, pmask = s->prefix_mask;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long start = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long rounds = (n + stride - 1) / stride;
+  const long long rounds = (n + stride * SEL_UNROLL - 1) / (stride * SEL_UNROLL);
   for (long long r = 0; r < rounds; r++) {
-    const long long i = start + r * stride;
-    int digit = -1;
-    if (i < n) {
-      const unsigned int key = __float_as_uint(v[i]);
-      if ((key & pmask) == prefix) digit = (int)((key >> shift) & (SEL_BINS - 1));
+    unsigned int key[SEL_UNROLL];
+    bool in[SEL_UNROLL];
+#pragma unroll
+    for (int u = 0; u < SEL_UNROLL; u++) {
+      const long long i = start + (r * SEL_UNROLL + u) * stride;
+      in[u] = i < n;
+      key[u] = in[u] ? __float_as_uint(v[i]) : 0u;
     }
-    const unsigned int peers = __match_any_sync(0xffffffffu, digit);
-    if (digit >= 0 && lane == __ffs(peers) - 1) atomicAdd(&h[warp][digit], (unsigned)__popc(peers));
+#pragma unroll
+    for (int u = 0; u < SEL_UNROLL; u++) {
+      const int digit = (in[u] && (key[u] & pmask) == prefix) ? (int)((key[u] >> shift) & (SEL_BINS - 1)) : -1;
+      if (__ballot_sync(0xffffffffu, digit >= 0) == 0u) continue;  // warp-uniform
+      const unsigned int peers = __match_any_sync(0xffffffffu, digit);
+      if (digit >= 0 && lane == __ffs(peers) - 1) atomicAdd(&h[warp][digit], (unsigned)__popc(peers));
+    }
   }
   __syncthreads();
   for (int d = threadIdx.x; d < SEL_BINS; d += blockDim.x) {
@@ -467,9 +499,22 @@ __global__ void mask_kernel(const float *__restrict__ v, const SelectState *stat
   const float t = use_rel ? __fmul_rn(s->result, rel_dev ? *rel_dev : rel) : s->result;
   v += (long long)b * n;
   flags += (long long)b * n;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const uint8_t f = flags[i];
-    flags[i] = (v[i] > t) ? (uint8_t)(f | FLAG_INSIDE) : (uint8_t)(f & ~FLAG_INSIDE);
+  // four elements per thread and round, their loads in flight together
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+    float x[4];
+    uint8_t f[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const long long i = i0 + u * stride;
+      x[u] = i < n ? v[i] : 0.0f;
+      f[u] = i < n ? flags[i] : (uint8_t)0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const long long i = i0 + u * stride;
+      if (i < n) flags[i] = (x[u] > t) ? (uint8_t)(f[u] | FLAG_INSIDE) : (uint8_t)(f[u] & ~FLAG_INSIDE);
+    }
   }
 }
 

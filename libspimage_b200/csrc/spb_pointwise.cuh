@@ -106,24 +106,27 @@ __device__ __forceinline__ float2 project(float2 G, long long idx, const PassArg
   return G;
 }
 
-// Fourier-domain Gaussian of sp_gaussian_blur (src/image_filter.c:80-90)
-__device__ __forceinline__ float2 gauss_mult(float2 F, long long gidx, const PassArgs &a) {
-  const long long idx = gidx % a.n_start;  // position within its start
-  const long long nxy = (long long)a.nx * a.ny;
-  const float z = (float)(idx / nxy);
-  const float y = (float)((idx % nxy) / a.nx);
-  const float x = (float)(idx % a.nx);
-  const float fx = (float)a.nx, fy = (float)a.ny, fz = (float)a.nz;
-  const float dx = (__fsub_rn(fx, x) < x) ? __fsub_rn(fx, x) : x;
-  const float dy = (__fsub_rn(fy, y) < y) ? __fsub_rn(fy, y) : y;
-  const float dz = (__fsub_rn(fz, z) < z) ? __fsub_rn(fz, z) : z;
+// Fourier-domain Gaussian of sp_gaussian_blur (src/image_filter.c:80-90):
+// the factor at distances (dx, dy, dz) of a pixel from the zero frequency
+// (each the smaller of x and n - x, an integer held in a float)
+__device__ __forceinline__ float gauss_factor(float dx, float dy, float dz, const PassArgs &a) {
   const double s = __dadd_rn(__dadd_rn(__dmul_rn((double)dx, (double)dx), __dmul_rn((double)dy, (double)dy)),
                              __dmul_rn((double)dz, (double)dz));
   const float dist = __double2float_rn(__dsqrt_rn(s));
   const float cr = __fdiv_rn(dist, a.nx_f);
   const double r2 = a.blur_r2_dev ? *a.blur_r2_dev : a.blur_r2;
   const double arg = __dmul_rn(__dmul_rn(a.blur_c0, __dmul_rn((double)cr, (double)cr)), r2);
-  const float m = __double2float_rn(__ddiv_rn(exp(arg), (double)a.n_f));
+  return __double2float_rn(__ddiv_rn(exp(arg), (double)a.n_f));
+}
+
+__device__ __forceinline__ float2 gauss_mult(float2 F, long long gidx, const PassArgs &a) {
+  const long long idx = gidx % a.n_start;  // position within its start
+  const long long nxy = (long long)a.nx * a.ny;
+  const int z = (int)(idx / nxy), y = (int)((idx % nxy) / a.nx), x = (int)(idx % a.nx);
+  const int dx = min(a.nx - x, x), dy = min(a.ny - y, y), dz = min(a.nz - z, z);
+  // the factor table of this blur (gauss_table_kernel) holds the same floats
+  const float m = a.blur_tab ? a.blur_tab[((long long)dz * (a.ny / 2 + 1) + dy) * (a.nx / 2 + 1) + dx]
+                             : gauss_factor((float)dx, (float)dy, (float)dz, a);
   return scale_cmul_dev(F, m);
 }
 
