@@ -6,9 +6,12 @@
  * p_drand48 over glibc rand()).
  */
 #include <math.h>
+#include <pthread.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include "spimage.h"
 
@@ -131,18 +134,104 @@ void sp_srand(int i) { srand((unsigned)i); }
 
 real p_drand48(void) { return (real)(((double)rand()) / (double)RAND_MAX); }
 
+/* n values of p_drand48() into out[], leaving the C library's rand() state
+ * exactly where n calls of rand() would leave it.  glibc's rand() is its
+ * random() generator: after srand() an additive feedback generator of degree
+ * 31 and separation 3 (x[i] = x[i-31] + x[i-3] mod 2^32, output x[i] >> 1).
+ * setstate() swaps in another state array and returns the current one, whose
+ * leading word then encodes the generator type (mod 5) and the position of
+ * its rear pointer (div 5).  When the current state has that form, the values
+ * are generated here (no lock and call per value) and the advanced state is
+ * handed back with setstate(); otherwise rand() is called n times. */
+static void drand_fill(real *out, long long n) {
+  enum { MAX_TYPES = 5, TYPE_3 = 3, DEG = 31, SEP = 3 };
+  static int32_t holder[DEG + 2]; /* leading word 0: a valid degree-0 state while ours is out */
+  int32_t *cur = (int32_t *)setstate((char *)holder);
+  if (cur) {
+    const int32_t word = cur[0];
+    if (word >= 0 && word % MAX_TYPES == TYPE_3 && word / MAX_TYPES < DEG) {
+      int32_t *x = cur + 1;
+      int r = word / MAX_TYPES, f = (r + SEP) % DEG;
+      for (long long i = 0; i < n; i++) {
+        const uint32_t val = (uint32_t)x[f] + (uint32_t)x[r];
+        x[f] = (int32_t)val;
+        out[i] = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
+        f = f + 1 == DEG ? 0 : f + 1;
+        r = r + 1 == DEG ? 0 : r + 1;
+      }
+      cur[0] = MAX_TYPES * r + TYPE_3;
+      setstate((char *)cur);
+      return;
+    }
+    setstate((char *)cur);
+  }
+  for (long long i = 0; i < n; i++) out[i] = p_drand48();
+}
+
+/* Random-phase rephasing, split so that the libm work runs on several host
+ * threads: the phases are drawn first, in pixel order from the one rand()
+ * sequence as the reference draws them; then each pixel's
+ * (cos(phase) * |v|, sin(phase) * |v|) is evaluated with the same double
+ * libm calls and roundings, on whichever thread -- the same bits. */
+typedef struct {
+  Complex *data;
+  const real *phase;
+  long long i0, i1;
+} rephase_span;
+
+static void *rephase_worker(void *arg) {
+  const rephase_span *s = (const rephase_span *)arg;
+  for (long long i = s->i0; i < s->i1; i++) {
+    const real phase = s->phase[i];
+    const real amp = sp_cabs(s->data[i]);
+    s->data[i].re = cos(phase) * amp;
+    s->data[i].im = sin(phase) * amp;
+  }
+  return NULL;
+}
+
+#define REPHASE_MAX_THREADS 32
+static void rephase_parallel(Complex *data, const real *phase, long long n) {
+  long long nt = n >= (1 << 16) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
+  if (nt < 1) nt = 1;
+  if (nt > REPHASE_MAX_THREADS) nt = REPHASE_MAX_THREADS;
+  pthread_t th[REPHASE_MAX_THREADS];
+  rephase_span span[REPHASE_MAX_THREADS];
+  int started[REPHASE_MAX_THREADS] = {0};
+  for (long long t = 0; t < nt; t++) {
+    span[t].data = data;
+    span[t].phase = phase;
+    span[t].i0 = n * t / nt;
+    span[t].i1 = n * (t + 1) / nt;
+    if (t > 0) started[t] = pthread_create(&th[t], NULL, rephase_worker, &span[t]) == 0;
+  }
+  rephase_worker(&span[0]);
+  for (long long t = 1; t < nt; t++) {
+    if (started[t]) pthread_join(th[t], NULL);
+    else rephase_worker(&span[t]); /* no thread: do the span here */
+  }
+}
+
 void sp_image_rephase(Image *img, int type) {
   img->phased = 1;
   const long long n = sp_image_size(img);
   if (type == SP_ZERO_PHASE) {
     for (long long i = 0; i < n; i++) img->image->data[i] = sp_cinit(sp_cabs(img->image->data[i]), 0);
   } else if (type == SP_RANDOM_PHASE) {
-    for (long long i = 0; i < n; i++) {
-      const real phase = p_drand48() * 3.14159265358979323846 * 2;
-      const real amp = sp_cabs(img->image->data[i]);
-      img->image->data[i].re = cos(phase) * amp;
-      img->image->data[i].im = sin(phase) * amp;
+    real *phase = (real *)malloc(sizeof(real) * (size_t)(n > 0 ? n : 1));
+    if (!phase) { /* no scratch: one pass, as the reference */
+      for (long long i = 0; i < n; i++) {
+        const real ph = p_drand48() * 3.14159265358979323846 * 2;
+        const real amp = sp_cabs(img->image->data[i]);
+        img->image->data[i].re = cos(ph) * amp;
+        img->image->data[i].im = sin(ph) * amp;
+      }
+      return;
     }
+    drand_fill(phase, n);
+    for (long long i = 0; i < n; i++) phase[i] = phase[i] * 3.14159265358979323846 * 2;
+    rephase_parallel(img->image->data, phase, n);
+    free(phase);
   }
 }
 

@@ -1,0 +1,62 @@
+"""Random-phase starts on the host (sp_image_rephase, the reference's
+src/image_util.c:1035-1067): the values come from the C library's rand()
+sequence and libm's double cos/sin exactly as the reference computes them
+one pixel at a time, although this library draws the sequence in bulk from
+the generator's state and evaluates cos/sin on several threads; and rand()
+continues afterwards as if it had been called once per pixel."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+SP_RANDOM_PHASE = 2
+RAND_MAX = 2147483647
+
+
+@pytest.fixture(scope="module")
+def env():
+    import libspimage_b200 as L
+
+    so = L.load()
+    so.sp_image_rephase.argtypes = [C.c_void_p, C.c_int]
+    libc = C.CDLL("libc.so.6")
+    libm = C.CDLL("libm.so.6")
+    for f in (libm.cos, libm.sin):
+        f.restype = C.c_double
+        f.argtypes = [C.c_double]
+    return L, so, libc, libm
+
+
+def _expected(libc, libm, amp, seed, skip):
+    """one rand() per pixel, cos/sin of the float phase in double, as the reference"""
+    libc.srand(seed)
+    for _ in range(skip):
+        libc.rand()
+    out = np.empty(amp.size, np.complex64)
+    for i, a in enumerate(amp.ravel()):
+        p = np.float32(float(libc.rand()) / RAND_MAX)
+        phase = np.float32(float(p) * 3.14159265358979323846 * 2)
+        av = float(np.sqrt(np.float32(a) * np.float32(a) + np.float32(0.0) * np.float32(0.0), dtype=np.float32))
+        out[i] = complex(np.float32(libm.cos(float(phase)) * av), np.float32(libm.sin(float(phase)) * av))
+    return out, libc.rand()
+
+
+@pytest.mark.parametrize("shape,seed,skip", [((16, 16), 3, 0), ((300, 300), 11, 5), ((1, 70001), 0, 31)])
+def test_rephase_matches_per_pixel_draws(env, shape, seed, skip):
+    L, so, libc, libm = env
+    amp = (np.random.default_rng(seed).random(shape) * 4).astype(np.float32)
+    img = L.new_image(amp.astype(np.complex64))
+    try:
+        libc.srand(seed)
+        for _ in range(skip):
+            libc.rand()
+        so.sp_image_rephase(C.cast(img, C.c_void_p), SP_RANDOM_PHASE)
+        after = libc.rand()
+        n = amp.size
+        fp = C.cast(img.contents.image.contents.data, C.POINTER(C.c_float))
+        got = np.ctypeslib.as_array(fp, shape=(2 * n,)).copy().view(np.complex64)
+    finally:
+        L.free_image(img)
+    exp, exp_after = _expected(libc, libm, amp, seed, skip)
+    assert np.array_equal(got.view(np.uint32), exp.view(np.uint32))
+    assert after == exp_after
