@@ -323,7 +323,9 @@ def batched_run(args, L, torch, world):
 
     from libspimage_b200 import replicas, synth
 
-    wl = WORKLOADS["batch512"]
+    wl = dict(WORKLOADS["batch512"])
+    if args.batch_starts:  # a smaller batch of the same job (profiling captures)
+        wl["starts"] = args.batch_starts
     nb = wl["starts"]
     n = int(np.prod(wl["shape"]))
     slots = slots_per_step(wl)
@@ -347,6 +349,13 @@ def batched_run(args, L, torch, world):
         if starts > 1:
             ef, _ = ph.starts_efourier()
             e0 = float(ef[0])
+            # then one support period with a CUDA event pair around every
+            # launch (direct launches) for the per-kernel rooflines
+            ph.profile(True)
+            assert ph.iterate(wl["period"]) == 0
+            torch.cuda.synchronize()
+            ktimes = ph.kernel_times()
+            ph.profile(False)
         else:
             e0 = ph.efourier()[0]
         res[label] = (ms, launches, e0)
@@ -364,6 +373,34 @@ def batched_run(args, L, torch, world):
                     "config": "the same job for one start (the batch's start 0), same pattern and schedule"}
     out["speedup_vs_plain"] = round(out["value"] / out["plain"]["value"], 3)
     out["efourier_final"] = {"batched_start0": bef, "plain": pef, "equal": bef == pef}
+    # HBM roofline: algorithmic bytes of each pass kernel over its live launch
+    # time, and of a whole iteration (support updates included) over the
+    # timed iteration rate
+    peak, peak_kind = measured_peak()
+    per_start = n * nb
+    kern = {}
+    for name, (nl, kms) in ktimes.items():
+        per_pixel = ALGO_BYTES_PER_PIXEL.get(name)
+        if per_pixel and nl:
+            avg_s = kms / nl / 1e3
+            tr = profiled_traffic(name, "batch512")
+            kern[name] = {"achieved": round(per_pixel * per_start / avg_s / 1e9, 1),
+                          "frac": round(per_pixel * per_start / avg_s / 1e9 / peak, 4),
+                          "avg_launch_us": round(avg_s * 1e6, 2),
+                          "algorithmic_bytes_per_launch": per_pixel * per_start,
+                          "traffic": tr * nb if tr else None}
+    it_s = bms / 1e3 / (args.batch_steps * slots)
+    it_bytes = sum(ALGO_BYTES_PER_PIXEL.values()) * per_start
+    dom = max(kern.items(), key=lambda kv: kv[1]["avg_launch_us"]) if kern else None
+    out["roofline"] = {"bound": "hbm", "kernel": dom[0] if dom else None,
+                       "achieved": dom[1]["achieved"] if dom else None, "peak": peak, "unit": "GB/s",
+                       "frac": dom[1]["frac"] if dom else None,
+                       "traffic": dom[1]["traffic"] if dom else None,
+                       "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)", "kernels": kern,
+                       "iteration": {"algorithmic_bytes": it_bytes, "ms": round(it_s * 1e3, 4),
+                                     "achieved": round(it_bytes / it_s / 1e9, 1),
+                                     "frac": round(it_bytes / it_s / 1e9 / peak, 4),
+                                     "note": "whole batch iteration incl. amortised support updates"}}
 
     # end to end through the C API with host buffers: amplitudes, mask and
     # support up, device-drawn starts, the whole job, every start's model and
@@ -713,6 +750,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=2, help="timed whole jobs of the batched block (0: skip it)")
     ap.add_argument("--batch-warm-slots", type=int, default=60)
+    ap.add_argument("--batch-starts", type=int, default=0, help="starts of the batched block (0: the workload's 512)")
     ap.add_argument("--batch-e2e-steps", type=int, default=1)
     ap.add_argument("--mixed-jobs", type=int, default=256, help="2-D jobs of the mixed batch (0: skip it)")
     ap.add_argument("--max-active-jobs", type=int, default=32)
