@@ -37,13 +37,18 @@ const char *spb_error_string(void);
 /* Number of usable CUDA devices (0 when there is none or the driver fails). */
 int spb_device_count(void);
 
-/* Self-check of the branch-free correctly rounded square root and quotient
- * that the projection passes use (no counterpart in the reference): compares
- * them bit for bit with the IEEE intrinsics on every float whose bit pattern
- * lies in [lo, hi) inside the square-root domain, and on ndiv pseudo-random
- * quotients drawn from seed; returns the mismatch counts (expected 0). */
+/* Self-check of the branch-free correctly rounded square root, reciprocal and
+ * quotient that the projection and support passes use (no counterpart in the
+ * reference): bit-for-bit comparisons with the IEEE intrinsics, counting
+ * differences into bad[4] (expected all 0): bad[0] square root and bad[1]
+ * reciprocal on every float whose bit pattern lies in [lo, hi) inside their
+ * domains; bad[2] on ndiv pseudo-random quotients drawn from seed; bad[3] on
+ * the quotients of pairs of significands in [1, 2): every divisor, the
+ * dividends of one residue class mod a_stride chosen per divisor from seed
+ * (a_stride 1: all 2^46 pairs; the calls with seed 0 .. a_stride-1 together
+ * also cover every pair; 0: skip). */
 int spb_check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
-                        unsigned long long *bad_sqrt, unsigned long long *bad_div);
+                        unsigned a_stride, unsigned long long *bad);
 
 /* Context for one nx*ny*nz problem on the current CUDA device; replaces the
  * device buffers the reference allocates in sp_phaser_set_amplitudes and

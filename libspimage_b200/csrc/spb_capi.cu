@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "spb_internal.h"
+#include "spb_pointwise.cuh"
 #include "spimage/spb_device.h"
 
 using namespace spb;
@@ -47,16 +48,15 @@ static int fail(const char *fmt, ...) {
 extern "C" const char *spb_error_string(void) { return g_err; }
 
 extern "C" int spb_check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
-                                   unsigned long long *bad_sqrt, unsigned long long *bad_div) {
-  unsigned long long *d = nullptr, h[2] = {0, 0};
+                                   unsigned a_stride, unsigned long long *bad) {
+  unsigned long long *d = nullptr, h[4] = {0, 0, 0, 0};
   if (cudaMalloc(&d, sizeof h) != cudaSuccess) return fail("cudaMalloc failed");
   cudaError_t e = cudaMemset(d, 0, sizeof h);
-  if (e == cudaSuccess) e = check_roundings(lo, hi, ndiv, seed, d);
+  if (e == cudaSuccess) e = check_roundings(lo, hi, ndiv, seed, a_stride, d);
   if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (e != cudaSuccess) return fail("rounding self-check: %s", cudaGetErrorString(e));
-  if (bad_sqrt) *bad_sqrt = h[0];
-  if (bad_div) *bad_div = h[1];
+  for (int k = 0; k < 4; k++) bad[k] = h[k];
   return 0;
 }
 
@@ -200,6 +200,7 @@ struct spb_ctx {
   float *gtab = nullptr;  // blur factor table, (nx/2+1)(ny/2+1)(nz/2+1)
   // line-major operands of the projection pass (lines along the last axis)
   float *amp_line = nullptr;
+  int *amp_bad = nullptr;  // set when an amplitude lies outside the branch-free quotient's domain
   uint32_t *meas_bits = nullptr;
   int proj_len = 0, meas_words = 0;
   long long proj_lines = 0, proj_estride = 0;
@@ -248,6 +249,7 @@ PassArgs base_args(const spb_ctx *c) {
   a.phased_amp = c->pamp;
   a.flags = c->flags;
   a.amp_line = c->amp_line;
+  a.amp_bad = c->amp_bad;
   a.meas_bits = c->meas_bits;
   a.meas_words = c->meas_words;
   a.row_lpb = c->tune[SPB_TUNE_ROW_LINES];
@@ -590,7 +592,7 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   if (c->st) cudaStreamSynchronize(c->st);
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
                   c->gp, c->T, c->absb, c->gtab, c->sel, c->red, c->ax.tw, c->ay.tw, c->az.tw,
-                  c->amp_line, c->meas_bits, c->beta_dev, c->beta_base, c->seeds, c->beta_zero, c->spar};
+                  c->amp_line, c->amp_bad, c->meas_bits, c->beta_dev, c->beta_base, c->seeds, c->beta_zero, c->spar};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : c->prof.ev) cudaEventDestroy(e);
@@ -672,13 +674,16 @@ static int download(spb_ctx *c, void *dst, const void *src, size_t bytes) {
 }
 
 namespace spb {
-// amp_line[L*len + i] = amp[i*estride + L]
+// amp_line[L*len + i] = amp[i*estride + L]; *bad = 1 if some amplitude is
+// neither zero nor of magnitude in [2^-60, 2^60] (the branch-free quotient's domain)
 __global__ void build_amp_line_kernel(const float *amp, float *amp_line, int len, long long estride,
-                                      long long nlines) {
+                                      long long nlines, int *bad) {
   const long long total = nlines * len;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
     const long long L = k / len, i = k % len;
-    amp_line[k] = amp[i * estride + L];
+    const float v = amp[i * estride + L];
+    amp_line[k] = v;
+    if (!div_rn_nb_domain(v)) *bad = 1;
   }
 }
 // bit i of line L = measured flag of pixel i*estride + L (of start 0)
@@ -733,7 +738,10 @@ static int proj_geometry(spb_ctx *c) {
 static int build_amp_line(spb_ctx *c) {
   if (!proj_geometry(c)) return 0;
   if (!c->amp_line) CK(cudaMalloc(&c->amp_line, sizeof(float) * (size_t)c->n));
-  build_amp_line_kernel<<<592, 256, 0, c->st>>>(c->amp, c->amp_line, c->proj_len, c->proj_estride, c->proj_lines);
+  if (!c->amp_bad) CK(cudaMalloc(&c->amp_bad, sizeof(int)));
+  CK(cudaMemsetAsync(c->amp_bad, 0, sizeof(int), c->st));
+  build_amp_line_kernel<<<592, 256, 0, c->st>>>(c->amp, c->amp_line, c->proj_len, c->proj_estride, c->proj_lines,
+                                                c->amp_bad);
   CK(cudaGetLastError());
   return 0;
 }

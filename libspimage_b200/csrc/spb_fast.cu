@@ -223,17 +223,18 @@ __device__ __forceinline__ void blur16(float2 (&v)[16], int col, long long o, in
 
 // Projection of a thread's 16 points (line index i = t + T*q) with the
 // line's amplitudes and measured bits in shared memory.  When every measured
-// point's |G|^2 lies in the domain of the branch-free square root and
-// quotient (the common case) the 16 projections contain no branch, so the
-// compiler interleaves them; otherwise the thread projects all 16 with the
-// IEEE intrinsics.  Both give the bits of project_with.
+// point's |G|^2 lies in the domain of the branch-free square root and every
+// amplitude in the quotient's (the common case) the 16 projections contain no
+// branch, so the compiler interleaves them; otherwise the thread projects all
+// 16 with the IEEE intrinsics.  Both give the bits of project_with.
 template <int T, bool FC>
 __device__ __forceinline__ void project16(float2 (&v)[16], const float *amp_l, const uint32_t *meas_l, int t,
                                           size_t lbase, size_t qstride, const PassArgs &a) {
   if (FC && (a.constraints & C_CENTROSYM))
 #pragma unroll
     for (int q = 0; q < 16; q++) v[q].y = 0.0f;
-  bool fast = a.objective == 0 && !(a.constraints & C_MARGIN);
+  // amp_bad: some amplitude lies outside the quotient's domain (set when the lines are built)
+  bool fast = a.objective == 0 && !(a.constraints & C_MARGIN) && a.amp_bad && !*a.amp_bad;
   float s2[16];
   unsigned mm = 0;
 #pragma unroll
@@ -487,19 +488,24 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
 }
 
 // ------------------------------------------- self-check of the roundings
-// Every float x in the square-root domain with bit pattern in [lo, hi), and
-// n pseudo-random quotients a/b with b in the quotient domain: counts the
-// results of the branch-free forms that differ in any bit from the IEEE
-// intrinsics'.
-__global__ void check_sqrt_kernel(unsigned lo, unsigned hi, unsigned long long *bad) {
-  unsigned long long nbad = 0;
+// Bit-for-bit comparisons of the branch-free forms with the IEEE intrinsics,
+// counting differences: every float x with bit pattern in [lo, hi) inside the
+// square-root domain (square root) and inside [2^-63, 2^63] (reciprocal);
+// n pseudo-random quotients a/b with a and b drawn over their domains; and the
+// quotients of significand pairs a in [1, 2) (every a_stride-th significand)
+// and b in [1, 2) (every significand; for divisor significand mb the
+// dividend's run over (mb * 2654435761 + seed) mod a_stride + k * a_stride, so
+// the calls with seed = 0 .. a_stride-1 cover every pair once).
+__global__ void check_sqrt_rcp_kernel(unsigned lo, unsigned hi, unsigned long long *bad) {
+  unsigned long long nsq = 0, nrc = 0;
   for (unsigned long long u = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; u < hi;
        u += (unsigned long long)gridDim.x * blockDim.x) {
     const float x = __uint_as_float((unsigned)u);
-    if (!sqrt_rn_nb_domain(x)) continue;
-    nbad += __float_as_uint(sqrt_rn_nb(x)) != __float_as_uint(__fsqrt_rn(x));
+    if (sqrt_rn_nb_domain(x)) nsq += __float_as_uint(sqrt_rn_nb(x)) != __float_as_uint(__fsqrt_rn(x));
+    if (x >= 0x1p-63f && x <= 0x1p63f) nrc += __float_as_uint(rcp_rn_nb(x)) != __float_as_uint(__frcp_rn(x));
   }
-  if (nbad) atomicAdd(bad, nbad);
+  if (nsq) atomicAdd(bad, nsq);
+  if (nrc) atomicAdd(bad + 1, nrc);
 }
 
 __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
@@ -514,21 +520,34 @@ __global__ void check_div_kernel(unsigned long long n, unsigned long long seed, 
   for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (unsigned long long)gridDim.x * blockDim.x) {
     const unsigned long long r = mix64(seed ^ mix64(k));
-    // a: any finite or non-finite pattern; b: exponent in [-63, 63), random sign-free significand
-    const float a = __uint_as_float((unsigned)r);
+    // a: random sign and significand, exponent in [-60, 60) (one in 64 draws: zero)
+    const unsigned ea = 67u + (unsigned)((r >> 24) % 120u);
+    const float a = ((r >> 58) == 0) ? 0.0f : __uint_as_float(((unsigned)r & 0x807FFFFFu) | (ea << 23));
+    // b: exponent in [-63, 63), random significand
     const unsigned eb = 64u + (unsigned)((r >> 32) % 126u);
     const float b = __uint_as_float((eb << 23) | ((unsigned)(r >> 40) & 0x7FFFFFu));
-    const float q = div_rn_nb(a, b), ref = __fdiv_rn(a, b);
-    const bool both_nan = isnan(q) && isnan(ref);
-    nbad += !both_nan && __float_as_uint(q) != __float_as_uint(ref);
+    nbad += __float_as_uint(div_rn_nb(a, b)) != __float_as_uint(__fdiv_rn(a, b));
+  }
+  if (nbad) atomicAdd(bad, nbad);
+}
+
+__global__ void check_div_significands_kernel(unsigned a_stride, unsigned phase, unsigned long long *bad) {
+  unsigned long long nbad = 0;
+  for (unsigned mb = blockIdx.x * blockDim.x + threadIdx.x; mb < (1u << 23); mb += gridDim.x * blockDim.x) {
+    const float b = __uint_as_float(0x3F800000u | mb);
+    for (unsigned ma = (mb * 2654435761u + phase) % a_stride; ma < (1u << 23); ma += a_stride) {
+      const float a = __uint_as_float(0x3F800000u | ma);
+      nbad += __float_as_uint(div_rn_nb(a, b)) != __float_as_uint(__fdiv_rn(a, b));
+    }
   }
   if (nbad) atomicAdd(bad, nbad);
 }
 
 cudaError_t check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
-                            unsigned long long *d_bad) {
-  check_sqrt_kernel<<<148 * 8, 256>>>(lo, hi, d_bad);
-  check_div_kernel<<<148 * 8, 256>>>(ndiv, seed, d_bad + 1);
+                            unsigned a_stride, unsigned long long *d_bad) {
+  if (hi > lo) check_sqrt_rcp_kernel<<<148 * 8, 256>>>(lo, hi, d_bad);
+  if (ndiv) check_div_kernel<<<148 * 8, 256>>>(ndiv, seed, d_bad + 2);
+  if (a_stride) check_div_significands_kernel<<<148 * 8, 256>>>(a_stride, (unsigned)(seed % a_stride), d_bad + 3);
   return cudaGetLastError();
 }
 

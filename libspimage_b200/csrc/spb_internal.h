@@ -68,6 +68,7 @@ struct PassArgs {
   // meas_bits[L*meas_words + i/32]; null when not built
   const float *amp_line;
   const uint32_t *meas_bits;
+  const int *amp_bad;  // nonzero: some amplitude of amp_line lies outside the branch-free quotient's domain
   int meas_words;
   // launch shape: lines per block of the row pass (0: the built-in choice)
   int row_lpb;
@@ -109,7 +110,7 @@ cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cud
 cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_gauss_table(const PassArgs &a, float *tab, cudaStream_t st);
 cudaError_t check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
-                            unsigned long long *d_bad);
+                            unsigned a_stride, unsigned long long *d_bad);
 
 // host-side launchers (spb_kernels.cu): register kernels where available,
 // general kernels otherwise

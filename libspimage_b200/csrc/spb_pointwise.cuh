@@ -32,28 +32,25 @@ __device__ __forceinline__ float2 apply_constraints(float2 g, uint8_t f, int c) 
 }
 
 // ---------------------------------------------------------------------------
-// Branch-free correctly rounded square root and quotient of floats.
-//
-// Method: evaluate the result in double precision to within one double ulp
-// (relative error < 2^-52), then round once to float.  A float square root or
-// quotient is never a float midpoint, and its distance from the nearest
-// midpoint is at least 2^-51 (square root) or 2^-49 (quotient) relative: the
-// midpoint M*2^e has an odd 25-bit M, so x - m^2 (resp. a - m*b) is a nonzero
-// multiple of the finer of the two grids.  A faithful double therefore lies on
-// the same side of every midpoint as the exact value and rounds to the
-// correctly rounded float (the double-rounding bound of S. Figueroa, "When is
-// double rounding innocuous?", SIGNUM Newsletter 30(3), 1995: p' >= 2p + 2).
-// The seeds are the hardware approximations of PTX rsqrt.approx.f32 (relative
-// error <= 2^-22.9) and rcp.approx.f32 (<= 1 ulp), refined by one Taylor step
-// in double:
-//   sqrt(x) = g (1 - r)^(-1/2) = g (1 + r/2 + 3r^2/8 + O(r^3)),  g = x t,  r = 1 - x t^2
-//   1/b     = t (1 - e)^(-1)   = t (1 + e + e^2 + O(e^3)),        e = 1 - b t
-// with |r|, |e| < 2^-21, so the truncation (< 2^-62) and the roundings of the
-// small terms are far below the last rounding.  Domain: x in [2^-126, 2^126]
-// (normal, with a normal reciprocal square root); b in [2^-63, 2^63]; a any
-// float (an infinite or NaN a propagates; an overflowing quotient rounds to
-// infinity as the IEEE quotient does).  Outside the domain the callers use
-// the IEEE intrinsics.
+// Branch-free correctly rounded square root, reciprocal and quotient of floats
+// (the bits of __fsqrt_rn, __frcp_rn and __fdiv_rn), from Newton-Raphson steps
+// with fused multiply-adds after P. Markstein, "Computation of elementary
+// functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1),
+// 1990, and "IA-64 and Elementary Functions" (2000), ch. 8:
+//  * square root: seed t ~ 1/sqrt(x) (PTX rsqrt.approx.f32, relative error
+//    <= 2^-22.9); g = x t, h = t/2; one coupled Newton step on (g, h) from the
+//    residual 1/2 - g h; then the final rounding g + (x - g^2) h, whose
+//    residual x - g^2 the fused multiply-add forms exactly;
+//  * reciprocal: seed y0 ~ 1/b (PTX rcp.approx.f32, <= 1 ulp); y = y0 + y0 (1 - b y0);
+//  * quotient: q0 = a y, one Newton correction q1 = q0 + (a - b q0) y, then
+//    Markstein's final rounding q1 + (a - b q1) y (exact residuals).
+// The square root and the reciprocal are checked bit for bit against the
+// intrinsics on every float of their domains, the quotient on every pair of
+// significands (spb_check_roundings; scaling by powers of two is exact inside
+// the domains).  Domains: x in [2^-96, 2^126] (below 2^-102 the residual
+// x - g^2 leaves the normal range and the square root misrounds); b in
+// [2^-63, 2^63]; a zero or with |a| in [2^-60, 2^60] (quotient and residuals
+// stay normal).  Outside them the callers use the intrinsics.
 __device__ __forceinline__ float rsqrt_seed(float x) {
   float t;
   asm("rsqrt.approx.f32 %0, %1;" : "=f"(t) : "f"(x));
@@ -64,20 +61,32 @@ __device__ __forceinline__ float rcp_seed(float x) {
   asm("rcp.approx.f32 %0, %1;" : "=f"(t) : "f"(x));
   return t;
 }
-__device__ __forceinline__ bool sqrt_rn_nb_domain(float x) { return x >= 0x1p-126f && x <= 0x1p126f; }
-__device__ __forceinline__ float sqrt_rn_nb(float x) {
-  const double X = (double)x, T = (double)rsqrt_seed(x);
-  const double G = X * T;                 // exact: 24 x 24 bits
-  const double R = fma(-G, T, 1.0);       // 1 - x t^2
-  const double H = R * fma(0.375, R, 0.5);
-  return __double2float_rn(fma(G, H, G));
+__device__ __forceinline__ bool sqrt_rn_nb_domain(float x) { return x >= 0x1p-96f && x <= 0x1p126f; }
+__device__ __forceinline__ bool div_rn_nb_domain(float a) {
+  const float m = fabsf(a);
+  return m == 0.0f || (m >= 0x1p-60f && m <= 0x1p60f);
 }
-// a / b for b in [2^-63, 2^63]
+__device__ __forceinline__ float sqrt_rn_nb(float x) {
+  const float t = rsqrt_seed(x);
+  float g = __fmul_rn(x, t);
+  float h = __fmul_rn(0.5f, t);
+  const float r = __fmaf_rn(-g, h, 0.5f);
+  g = __fmaf_rn(g, r, g);
+  h = __fmaf_rn(h, r, h);
+  const float d = __fmaf_rn(-g, g, x);
+  return __fmaf_rn(d, h, g);
+}
+// 1/b for b in [2^-63, 2^63]
+__device__ __forceinline__ float rcp_rn_nb(float b) {
+  const float y0 = rcp_seed(b);
+  return __fmaf_rn(__fmaf_rn(-b, y0, 1.0f), y0, y0);
+}
+// a / b for b in [2^-63, 2^63] and a in div_rn_nb_domain
 __device__ __forceinline__ float div_rn_nb(float a, float b) {
-  const double B = (double)b, T = (double)rcp_seed(b);
-  const double E = fma(-B, T, 1.0);       // 1 - b t, exact (Sterbenz)
-  const double Y = fma(T, fma(E, E, E), T);
-  return __double2float_rn((double)a * Y);
+  const float y = rcp_rn_nb(b);
+  const float q0 = __fmul_rn(a, y);
+  const float q1 = __fmaf_rn(__fmaf_rn(-b, q0, a), y, q0);
+  return __fmaf_rn(__fmaf_rn(-b, q1, a), y, q1);
 }
 
 // Fourier-space projection at pixel idx (src/phasing.c:1061-1109)
