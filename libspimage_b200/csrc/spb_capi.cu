@@ -1103,6 +1103,7 @@ extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float 
   a.gamma2 = alg->gamma2;
   a.one_p_g2 = 1 + alg->gamma2;
   a.size_f = (float)(int)c->n;
+  a.inv_size_pow2 = (c->n & (c->n - 1)) == 0 ? (float)(1.0 / (double)c->n) : 0.0f;
   // a short call (one support period, typically) runs as one captured graph
   if (c->use_graphs && !c->prof.on && c->warm_alg[A] && iterations >= 2 && iterations <= kWholeGraphMax) {
     GraphEntry *g = find_graph(c, alg, iterations, keep_gp);
@@ -1466,7 +1467,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   for (int cand = 0; cand < 2 * 2 * 16 && !rc; cand++) {
     const int nopdl = cand & 1, g0 = 1 + ((cand >> 1) & 1), li = cand >> 2;
     const int lines = li ? 1 << (li - 1) : 0;
-    if (lines >= lpb_max) continue;  // lpb_max is the built-in choice (0)
+    if (lines > lpb_max) continue;  // (0 is the built-in choice, which may be lpb_max or fewer)
     {
       if (apply_choice(c, TuneChoice{lines, nopdl, g0})) {
         rc = -1;

@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
   float2 *g0_s = sm + ((N + lpb * S + 1) & ~1);
   uint8_t *fl_s = reinterpret_cast<uint8_t *>(g0_s + (G0LATE ? 0 : lpb * N));
   const int vrows = min(lpb, nrows - row0);
-  if constexpr (MODE == ROW_ITER) {
+  if constexpr (MODE == ROW_ITER || MODE == ROW_DM_ITER) {
     // g0 (unless G0LATE) and flags of this block's rows: contiguous, copied in 16-byte chunks
     if constexpr (!G0LATE) {
       const float2 *g0src = a.g0 + (size_t)row0 * N;
@@ -309,9 +309,11 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
   }
   pdl_wait();
   float2 v[16];
+  float2 w[MODE == ROW_DM_ITER ? 16 : 1];  // the difference map's second line (Yf)
 #pragma unroll
   for (int q = 0; q < 16; q++) {
     float2 x = make_float2(0.0f, 0.0f);
+    if constexpr (MODE == ROW_DM_ITER) w[q] = valid ? a.src2[base + T * q] : x;
     if (valid) {
       const size_t idx = base + T * q;
       if constexpr (MODE == ROW_FWD_F32) x = make_float2(a.f32src[idx], 0.0f);
@@ -402,6 +404,61 @@ __global__ void __launch_bounds__(256) row_fast_kernel(PassArgs a, const float2 
     if (valid)
 #pragma unroll
       for (int q = 0; q < 16; q++) a.dst[base + T * q] = v[q];
+  } else if constexpr (MODE == ROW_DM_ITER) {
+    // difference map (src/phasing.c:1111-1168 as restated by the general row
+    // pass): inverse x of Y and Yf, the update of g and f1, forward x of both
+    const float beta = iter_beta(a);
+    reg::fft<N, true>(v, line, t, tw_s);
+    reg::fft<N, true>(w, line, t, tw_s);
+    if constexpr (G0LATE) {
+      const float2 *g0src = a.g0 + (size_t)row0 * N;
+      for (int c = threadIdx.x; c < vrows * (N / 2); c += blockDim.x) {
+        const int r = c / (N / 2), j = c % (N / 2);
+        if constexpr (S % 2 == 0) cp_async16(sm + N + r * S + 2 * j, g0src + (size_t)r * N + 2 * j);
+        else {
+          cp_async8(sm + N + r * S + 2 * j, g0src + (size_t)r * N + 2 * j);
+          cp_async8(sm + N + r * S + 2 * j + 1, g0src + (size_t)r * N + 2 * j + 1);
+        }
+      }
+      cp_async_wait_all();
+      __syncthreads();
+    }
+    const float2 *g0r = G0LATE ? line + t : g0_s + lr * N + t;
+    const uint8_t *flr = fl_s + lr * N + t;
+    // x / size as the reference divides; a multiply by the exact reciprocal when the size is a power of two
+    auto div_size = [&](float x) { return a.inv_size_pow2 != 0.0f ? fmul(x, a.inv_size_pow2) : __fdiv_rn(x, a.size_f); };
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      float2 g = make_float2(0.0f, 0.0f), f1 = g;
+      if (valid) {
+        const float2 rv = v[q], fv = w[q], g0 = g0r[T * q];
+        if (a.gp) a.gp[base + T * q] = rv;
+        const uint8_t f = flr[T * q];
+        if (f & FLAG_INSIDE) {
+          g.x = fadd(g0.x, fmul(beta, fsub(div_size(fmul(a.one_p_g2, rv.x)), fmul(a.gamma2, g0.x))));
+          g.y = fadd(g0.y, fmul(beta, fsub(div_size(fmul(a.one_p_g2, rv.y)), fmul(a.gamma2, g0.y))));
+        } else {
+          g = g0;
+        }
+        g.x = fsub(g.x, div_size(fmul(beta, fv.x)));
+        g.y = fsub(g.y, div_size(fmul(beta, fv.y)));
+        g = apply_constraints(g, f, a.constraints);
+        a.g1[base + T * q] = g;
+        f1 = (f & FLAG_INSIDE) ? g : make_float2(fmul(-a.gamma1, g.x), fmul(-a.gamma1, g.y));
+      }
+      v[q] = g;
+      w[q] = f1;
+    }
+    if constexpr (G0LATE) __syncthreads();  // every g0 read done before the forward transforms write the lines
+    reg::fft<N, false>(v, line, t, tw_s);
+    reg::fft<N, false>(w, line, t, tw_s);
+    pdl_release();
+    if (valid)
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        a.dst[base + T * q] = v[q];
+        a.dst2[base + T * q] = w[q];
+      }
   }
 }
 
@@ -574,19 +631,27 @@ template <int N, int MODE>
 static cudaError_t row_fast_launch(const LinePlan &px, const PassArgs &a, cudaStream_t st) {
   constexpr int T = N / 16;
   constexpr int LPB_MAX = (256 / T) > 0 ? (256 / T) : 1;  // 256 threads per block at most
-  const int LPB = (a.row_lpb > 0 && a.row_lpb < LPB_MAX) ? a.row_lpb : LPB_MAX;
   const long long nrows = a.n / N;
+  static int nsm = 0;
+  if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) return cudaGetLastError();
+  // a few short difference-map rows per SM: the general row pass (one
+  // butterfly per thread, more threads per row) is faster
+  if (MODE == ROW_DM_ITER && N < 256 && nrows < 4LL * nsm) return cudaErrorNotSupported;
+  int LPB = (a.row_lpb > 0 && a.row_lpb < LPB_MAX) ? a.row_lpb : LPB_MAX;
+  if (a.row_lpb <= 0) {
+    // built-in choice: 256 threads per block, fewer (down to one warp) while
+    // the grid would leave SMs without a block
+    while (LPB > 1 && LPB * T > 32 && (nrows + LPB - 1) / LPB < nsm) LPB >>= 1;
+  }
   const long long grid = (nrows + LPB - 1) / LPB;
   const size_t smem0 = (size_t)((N + LPB * (N + N / 16) + 1) & ~1) * sizeof(float2);
-  if constexpr (MODE == ROW_ITER) {
+  if constexpr (MODE == ROW_ITER || MODE == ROW_DM_ITER) {
     // g0 staging: SPB_TUNE_ROW_G0 1 = at the start, 2 = between the
     // transforms; 0 = between the transforms when the grid is larger than the
     // blocks that fit on the device at once with the larger staging
     const size_t smem_early = smem0 + (size_t)LPB * N * (sizeof(float2) + 1), smem_late = smem0 + (size_t)LPB * N;
     bool late = a.row_g0 == 2;
     if (a.row_g0 == 0) {
-      static int nsm = 0;
-      if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) return cudaGetLastError();
       int per_sm = 0;
       cudaError_t e = ensure_smem<row_fast_kernel<N, MODE, false>>(smem_early);
       if (e == cudaSuccess)
@@ -655,6 +720,7 @@ static cudaError_t row_fast_mode(int mode, const LinePlan &px, const PassArgs &a
     case ROW_INV_SCALE: return row_fast_launch<N, ROW_INV_SCALE>(px, a, st);
     case ROW_INV_ABS: return row_fast_launch<N, ROW_INV_ABS>(px, a, st);
     case ROW_ITER: return row_fast_launch<N, ROW_ITER>(px, a, st);
+    case ROW_DM_ITER: return row_fast_launch<N, ROW_DM_ITER>(px, a, st);
     case ROW_FWD_F32: return row_fast_launch<N, ROW_FWD_F32>(px, a, st);
     case ROW_FWD_SQUARE_F32: return row_fast_launch<N, ROW_FWD_SQUARE_F32>(px, a, st);
   }

@@ -83,6 +83,7 @@ struct PassArgs {
   const int *beta_base;
   int beta_idx;
   float gamma1, gamma2, one_p_g2, size_f;
+  float inv_size_pow2;  // 1/size_f when the image size is a power of two (x/size_f == x*inv_size_pow2 then), else 0
   // pixels per start: the amplitude-side arrays (amp, amp_min, amp_max,
   // phased_amp) hold one start and are indexed modulo n_start
   long long n_start;

@@ -76,6 +76,11 @@ SCENARIOS = [
     ("hio_area_192", (192, 192), HIO, [(AREA, 7, 2.0, 0.1)], 2),
     ("raar_thr_1000", (24, 1000), RAAR, [(THRESHOLD, 6, 2.0, 0.2)], 2),
     ("er_area_384", (384, 48), ER, [(AREA, 5, 1.5, 0.1)], 2),
+    # difference map: register row pass (power-of-two rows) and general row pass
+    ("dm_area_256", (128, 256), DIFFMAP, [(AREA, 9, 2.0, 0.1)], 2),
+    ("dm_area_3d", (16, 16, 32), DIFFMAP, [(AREA, 5, 2.0, 0.1)], 2),
+    ("dm_48", (40, 48), DIFFMAP, None, 2),
+    ("dm_many_short_rows", (640, 32), DIFFMAP, [(AREA, 7, 2.0, 0.1)], 2),
 ]
 
 
@@ -198,7 +203,7 @@ def test_close_centre_batched_starts(lib):
         assert same_bits(batch.start_model(b), one.model())
 
 
-@pytest.mark.parametrize("shape,alg,sup", [((256, 256), HIO, [(AREA, 20, 3.0, 0.05)]), ((64, 48), DIFFMAP, None),
+@pytest.mark.parametrize("shape,alg,sup", [((256, 256), HIO, [(AREA, 20, 3.0, 0.05)]), ((64, 64), DIFFMAP, None),
                                            ((16, 16, 16), RAAR, [(AREA, 10, 2.0, 0.1)])])
 def test_autotune_and_launch_shapes_leave_results_unchanged(lib, oracle_mod, shape, alg, sup):
     """the autotuner restores the reconstruction it times on, and every
