@@ -30,6 +30,12 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
   float2 *B = A + slab;
   float2 *Cb = A + 2 * slab;
   float2 *D = A + 3 * slab;
+  // the update's operands, loaded with the line: g0 after the transform
+  // buffers, then the flags (bytes)
+  constexpr bool UPD = (MODE == ROW_ITER || MODE == ROW_DM_ITER);
+  constexpr int NBUF = (MODE == ROW_DM_ITER) ? 4 : 2;
+  float2 *G0S = smem + (size_t)NBUF * slab + (size_t)lr * n;
+  uint8_t *FLS = reinterpret_cast<uint8_t *>(smem + (size_t)(NBUF + 1) * slab) + (size_t)lr * n;
 
   for (int i = t; i < n; i += tpr) {
     float2 v = make_float2(0.0f, 0.0f), w = make_float2(0.0f, 0.0f);
@@ -51,6 +57,12 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
     }
     A[i] = v;
     if constexpr (MODE == ROW_DM_ITER) Cb[i] = w;
+    if constexpr (UPD) {
+      if (valid) {
+        G0S[i] = a.g0[base + i];
+        FLS[i] = a.flags[base + i];
+      }
+    }
   }
   __syncthreads();
 
@@ -78,14 +90,14 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
         const long long idx = base + i;
         const float2 gp = scale_cmul_dev(r[i], a.inv_n);
         if (a.gp) a.gp[idx] = gp;
-        const uint8_t f = a.flags[idx];
+        const uint8_t f = FLS[i];
         if (f & FLAG_INSIDE) {
           g = gp;
         } else if (a.alg == ALG_HIO) {
-          const float2 g0 = a.g0[idx];
+          const float2 g0 = G0S[i];
           g = make_float2(fsub(g0.x, fmul(gp.x, beta)), fsub(g0.y, fmul(gp.y, beta)));
         } else if (a.alg == ALG_RAAR) {
-          const float2 g0 = a.g0[idx];
+          const float2 g0 = G0S[i];
           g = make_float2(fadd(fmul(gp.x, one_m2b), fmul(g0.x, beta)),
                           fadd(fmul(gp.y, one_m2b), fmul(g0.y, beta)));
         }
@@ -107,9 +119,9 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
       float2 g = make_float2(0.0f, 0.0f), f1 = g;
       if (valid) {
         const long long idx = base + i;
-        const float2 rv = rho[i], fv = fr[i], g0 = a.g0[idx];
+        const float2 rv = rho[i], fv = fr[i], g0 = G0S[i];
         if (a.gp) a.gp[idx] = rv;
-        const uint8_t f = a.flags[idx];
+        const uint8_t f = FLS[i];
         if (f & FLAG_INSIDE) {
           g.x = fadd(g0.x, fmul(beta, fsub(__fdiv_rn(fmul(a.one_p_g2, rv.x), a.size_f), fmul(a.gamma2, g0.x))));
           g.y = fadd(g0.y, fmul(beta, fsub(__fdiv_rn(fmul(a.one_p_g2, rv.y), a.size_f), fmul(a.gamma2, g0.y))));
@@ -150,6 +162,12 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
   float2 *A = smem + cc;
   float2 *B = smem + (size_t)n * ct + cc;
   const long long lbase = o * a.ostride + c;
+  // projection operands, loaded with the line: amplitudes after the two
+  // transform buffers, then the flags (bytes); ai0 = amplitude index of element 0
+  constexpr bool PROJ = (MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC);
+  float *AMc = reinterpret_cast<float *>(smem + (size_t)2 * n * ct) + cc;
+  uint8_t *FLc = reinterpret_cast<uint8_t *>(reinterpret_cast<float *>(smem + (size_t)2 * n * ct) + (size_t)n * ct) + cc;
+  const long long ai0 = PROJ ? lbase % a.n_start : 0;
 
   for (int i = t; i < n; i += tpc) {
     float2 v = make_float2(0.0f, 0.0f);
@@ -159,6 +177,10 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
         v = make_float2(fmul(s, s), 0.0f);
       } else {
         v = a.src[lbase + i * a.estride];
+      }
+      if constexpr (PROJ) {
+        AMc[(size_t)i * ct] = a.amp[ai0 + i * a.estride];
+        FLc[(size_t)i * ct] = a.flags[lbase + i * a.estride];
       }
     }
     A[(size_t)i * ct] = v;
@@ -176,8 +198,8 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
       for (int i = t; i < n; i += tpc) {
         const long long idx = lbase + i * a.estride;
         float2 G = f[(size_t)i * ct];
-        if constexpr (MODE == COL_PROJECT) G = project(G, idx, a, true);
-        else if constexpr (MODE == COL_PROJECT_NOFC) G = project(G, idx, a, false);
+        if constexpr (PROJ)
+          G = project_vals(G, FLc[(size_t)i * ct], AMc[(size_t)i * ct], ai0 + i * a.estride, a, MODE == COL_PROJECT);
         else G = gauss_mult(G, idx, a);
         f[(size_t)i * ct] = G;
       }
@@ -227,7 +249,9 @@ static cudaError_t row_launch_n(const LinePlan &px, const PassArgs &a, cudaStrea
     if (cap < rpb) rpb = cap > 0 ? (int)cap : 1;
   }
   const int nbuf = (MODE == ROW_DM_ITER) ? 4 : 2;
-  const size_t smem = (size_t)nbuf * rpb * n * sizeof(float2);
+  constexpr bool UPD = (MODE == ROW_ITER || MODE == ROW_DM_ITER);
+  // transform buffers, then (UPD) a slab of g0 and rpb*n bytes of flags
+  const size_t smem = (size_t)(nbuf + (UPD ? 1 : 0)) * rpb * n * sizeof(float2) + (UPD ? (size_t)rpb * n : 0);
   auto k = row_pass_kernel<MODE, NC>;
   static size_t done = 0;
   cudaError_t e = smem_attr(k, smem, done);
@@ -286,7 +310,9 @@ static cudaError_t col_launch_n(const LinePlan &pl, const PassArgs &a, cudaStrea
   if (NC > 0 && tpc * ct > 1024) ct = 1024 / tpc > 0 ? 1024 / tpc : 1;  // keep one butterfly per thread
   if (tpc * ct > 1024) tpc = 1024 / ct;
   if (tpc * ct < 32) tpc = 32 / ct;
-  const size_t smem = (size_t)2 * n * ct * sizeof(float2);
+  constexpr bool PROJ = (MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC);
+  // two transform buffers, then (projection) n*ct amplitudes and n*ct flag bytes
+  const size_t smem = (size_t)2 * n * ct * sizeof(float2) + (PROJ ? (size_t)n * ct * (sizeof(float) + 1) : 0);
   auto k = col_pass_kernel<MODE, NC>;
   static size_t done = 0;
   cudaError_t e = smem_attr(k, smem, done);

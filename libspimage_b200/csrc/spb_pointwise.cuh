@@ -89,17 +89,19 @@ __device__ __forceinline__ float div_rn_nb(float a, float b) {
   return __fmaf_rn(__fmaf_rn(-b, q1, a), y, q1);
 }
 
-// Fourier-space projection at pixel idx (src/phasing.c:1061-1109)
-__device__ __forceinline__ float2 project(float2 G, long long idx, const PassArgs &a, bool fourier_constraints) {
-  const uint8_t f = a.flags[idx];
-  const long long ai = idx % a.n_start;  // amplitude-side arrays hold one start
+// Fourier-space projection (src/phasing.c:1061-1109) of G with the pixel's
+// flags f and amplitude amp (ai: its index within a start)
+__device__ __forceinline__ float2 project_vals(float2 G, uint8_t f, float amp, long long ai, const PassArgs &a,
+                                               bool fourier_constraints) {
   if (fourier_constraints && (a.constraints & C_CENTROSYM)) G.y = 0.0f;
   if (a.objective == 0) {
     if (f & FLAG_MEASURED) {
       float m = 1.0f;
-      const float amp = a.amp[ai];
       if (!(a.constraints & C_MARGIN)) {
-        m = __fdiv_rn(amp, cabs_ref(G));
+        // amp / |G|, |G| = sqrt(im*im + re*re) rounded once (cabs_ref)
+        const float s2 = fadd(fmul(G.y, G.y), fmul(G.x, G.x));
+        m = (sqrt_rn_nb_domain(s2) && div_rn_nb_domain(amp)) ? div_rn_nb(amp, sqrt_rn_nb(s2))
+                                                             : __fdiv_rn(amp, __fsqrt_rn(s2));
       } else {
         const float av = cabs_ref(G);
         const float lo = a.amp_min[ai], hi = a.amp_max[ai];
@@ -113,6 +115,12 @@ __device__ __forceinline__ float2 project(float2 G, long long idx, const PassArg
     if (f & FLAG_MEASURED) G = a.phased_amp[ai];
   }
   return G;
+}
+
+// the same at pixel idx, operands read from global memory
+__device__ __forceinline__ float2 project(float2 G, long long idx, const PassArgs &a, bool fourier_constraints) {
+  const long long ai = idx % a.n_start;  // amplitude-side arrays hold one start
+  return project_vals(G, a.flags[idx], a.amp[ai], ai, a, fourier_constraints);
 }
 
 // Fourier-domain Gaussian of sp_gaussian_blur (src/image_filter.c:80-90):
