@@ -204,6 +204,7 @@ def test_close_centre_batched_starts(lib):
 
 
 @pytest.mark.parametrize("shape,alg,sup", [((256, 256), HIO, [(AREA, 20, 3.0, 0.05)]), ((64, 64), DIFFMAP, None),
+                                           ((640, 32), DIFFMAP, [(AREA, 7, 2.0, 0.1)]),
                                            ((16, 16, 16), RAAR, [(AREA, 10, 2.0, 0.1)])])
 def test_autotune_and_launch_shapes_leave_results_unchanged(lib, oracle_mod, shape, alg, sup):
     """the autotuner restores the reconstruction it times on, and every
