@@ -753,8 +753,9 @@ def main():
     ap.add_argument("--batch-starts", type=int, default=0, help="starts of the batched block (0: the workload's 512)")
     ap.add_argument("--batch-e2e-steps", type=int, default=1)
     ap.add_argument("--mixed-jobs", type=int, default=256, help="2-D jobs of the mixed batch (0: skip it)")
-    ap.add_argument("--max-active-jobs", type=int, default=16,
-                    help="server admission limit (16 measured best for the mixed batch: 16/32/64/96 -> 59.5k/56.5k/45.2k/50.3k)")
+    ap.add_argument("--max-active-jobs", type=int, default=8,
+                    help="server admission limit; mixed batch, start-iterations/s by limit on three boxes: "
+                         "4/6/8: 67.9k/69.2k/63.6k; 8/12/16/24: 69.7k/63.1k/64.5k/50.9k; 16/32/64/96: 59.5k/56.5k/45.2k/50.3k")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="offered arrivals per second")
     ap.add_argument("--serve-window", type=float, default=1.0, help="seconds of arrivals (0: skip serving)")
     ap.add_argument("--serve-sustained-window", type=float, default=5.0)

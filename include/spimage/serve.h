@@ -31,7 +31,7 @@ typedef struct spb_server spb_server;
 
 typedef struct {
   double hbm_budget_bytes; /* device memory for job contexts; 0: 60% of the free memory at creation */
-  int max_active_jobs;     /* jobs on the GPU at once; 0: 16 */
+  int max_active_jobs;     /* jobs on the GPU at once; 0: 8 */
   int chunk_slots;         /* iteration slots per enqueued chunk; 0: 100 */
   int chunks_ahead;        /* chunks queued per job ahead of the GPU; 0: 2 */
   int no_autotune;         /* 1: keep the built-in launch shapes; 0: tune them (sp_phaser_autotune) for the

@@ -478,7 +478,7 @@ extern "C" int spb_server_create(spb_server **out, const spb_server_config *cfg)
     }
     s->cfg.hbm_budget_bytes = 0.6 * (double)fr;
   }
-  if (s->cfg.max_active_jobs <= 0) s->cfg.max_active_jobs = 16;
+  if (s->cfg.max_active_jobs <= 0) s->cfg.max_active_jobs = 8;
   if (s->cfg.chunk_slots <= 0) s->cfg.chunk_slots = 100;
   if (s->cfg.chunks_ahead <= 0) s->cfg.chunks_ahead = 2;
   s->t0 = Clock::now();
