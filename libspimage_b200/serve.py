@@ -1,6 +1,6 @@
 """ctypes binding of the reconstruction server (include/spimage/serve.h).
 
-    srv = Server(max_active_jobs=16)
+    srv = Server(max_active_jobs=8)
     jid = srv.submit(amp, mask, support, stages=[(SpHIO, 0.9, 1000), (SpER, 0.0, 100)],
                      starts=8, seed=0, support_period=20, area=0.05, blur=(3.0, 0.7))
     info = srv.wait(jid)            # dict with status and timestamps
