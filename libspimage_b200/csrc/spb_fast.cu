@@ -12,6 +12,12 @@
 // that every exchange is free of bank conflicts.  Twiddles are read from a
 // per-stage table laid out [stage][m-1][k] (consecutive k for consecutive
 // threads), holding the very same float values as the per-length table.
+//
+// Row kernels: forward/inverse/|.| transforms, the HIO/RAAR/ER iteration
+// (inverse x, update, forward x) and the difference map's iteration (two
+// lines per row: inverse x of Y and Yf, the update, forward x of g and f1).
+// Column kernels: transforms, the Fourier projection with line-major
+// amplitudes and measured bits, the blur multiplier.
 #include <math.h>
 
 #include "spb_internal.h"

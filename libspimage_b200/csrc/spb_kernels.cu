@@ -231,8 +231,9 @@ static cudaError_t smem_attr(K k, size_t smem, size_t &done) {
 // lengths with a compile-time plan in the general kernels (the non-power-of-two
 // sizes of the mixed batches); others use the run-time plan
 #define SPB_CT_LENGTHS(X) X(192) X(384) X(1000)
-// the difference map's row passes have no register kernel: compile-time plans
-// for the power-of-two lengths too
+// the difference map's row passes also take compile-time plans at powers of
+// two: grids of a few short rows per SM run here rather than in the register
+// kernel (spb_fast.cu), and so does the f1 transform (ROW_DM_F1_FWD)
 #define SPB_CT_LENGTHS_DM(X) X(64) X(128) X(256) X(512) X(1024) X(2048)
 
 template <int MODE, int NC>
