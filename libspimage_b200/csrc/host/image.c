@@ -142,7 +142,11 @@ real p_drand48(void) { return (real)(((double)rand()) / (double)RAND_MAX); }
  * leading word then encodes the generator type (mod 5) and the position of
  * its rear pointer (div 5).  When the current state has that form, the values
  * are generated here (no lock and call per value) and the advanced state is
- * handed back with setstate(); otherwise rand() is called n times. */
+ * handed back with setstate(); otherwise rand() is called n times.  Other
+ * threads that call rand() or srand() meanwhile act on a stand-in state (the
+ * drawn values and the final state are the ones above): such concurrent use
+ * interleaves unpredictably with a per-value rand() loop too.  No thread of
+ * this library calls rand() (the server draws its starts on the device). */
 static void drand_fill(real *out, long long n) {
   enum { MAX_TYPES = 5, TYPE_3 = 3, DEG = 31, SEP = 3 };
   static int32_t holder[DEG + 2]; /* leading word 0: a valid degree-0 state while ours is out */
