@@ -398,6 +398,24 @@ class Phaser:
     def fmodel(self):
         return self._get(self.lib.sp_phaser_fmodel)
 
+    def _get_masked(self, fn):
+        img = fn(self.ph)
+        if not img:
+            raise RuntimeError(self.lib.sp_phaser_last_error().decode())
+        return image_data(img, self.shape), image_mask(img, self.shape)
+
+    def fmodel_with_mask(self):
+        """(FFT of the model, measured-amplitude mask)"""
+        return self._get_masked(self.lib.sp_phaser_fmodel_with_mask)
+
+    def model_with_support(self):
+        """(model, support as mask)"""
+        return self._get_masked(self.lib.sp_phaser_model_with_support)
+
+    def amplitudes_image(self):
+        """(amplitudes as a complex image, measured mask)"""
+        return self._get_masked(self.lib.sp_phaser_amplitudes)
+
     def support(self):
         img = self.lib.sp_phaser_support(self.ph)
         return (image_data(img, self.shape).real != 0).astype(np.int32)

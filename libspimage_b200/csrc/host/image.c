@@ -142,16 +142,27 @@ real p_drand48(void) { return (real)(((double)rand()) / (double)RAND_MAX); }
  * leading word then encodes the generator type (mod 5) and the position of
  * its rear pointer (div 5).  When the current state has that form, the values
  * are generated here (no lock and call per value) and the advanced state is
- * handed back with setstate(); otherwise rand() is called n times.  Other
- * threads that call rand() or srand() meanwhile act on a stand-in state (the
- * drawn values and the final state are the ones above): such concurrent use
- * interleaves unpredictably with a per-value rand() loop too.  No thread of
- * this library calls rand() (the server draws its starts on the device). */
+ * handed back with setstate(); otherwise rand() is called n times.
+ *
+ * Two bulk draws never overlap: a process-wide mutex covers the span from
+ * the first setstate() to the restoring one, so a second draw cannot take
+ * the stand-in state for the real one and leave the generator on it.  If
+ * setstate() nevertheless hands back the stand-in (another caller swapped
+ * it in), the real state is not ours to restore and the per-value loop is
+ * used.  Outside callers of rand()/srand() during a bulk draw act on the
+ * stand-in (the drawn values and the final state are the ones above); such
+ * concurrent use interleaves unpredictably with a per-value rand() loop
+ * too.  The state layout is glibc's: other C libraries take the per-value
+ * loop.  No thread of this library calls rand() (the server draws its
+ * starts on the device). */
 static void drand_fill(real *out, long long n) {
+#if defined(__GLIBC__)
   enum { MAX_TYPES = 5, TYPE_3 = 3, DEG = 31, SEP = 3 };
+  static pthread_mutex_t mu = PTHREAD_MUTEX_INITIALIZER;
   static int32_t holder[DEG + 2]; /* leading word 0: a valid degree-0 state while ours is out */
+  pthread_mutex_lock(&mu);
   int32_t *cur = (int32_t *)setstate((char *)holder);
-  if (cur) {
+  if (cur && cur != holder) {
     const int32_t word = cur[0];
     if (word >= 0 && word % MAX_TYPES == TYPE_3 && word / MAX_TYPES < DEG) {
       int32_t *x = cur + 1;
@@ -165,10 +176,13 @@ static void drand_fill(real *out, long long n) {
       }
       cur[0] = MAX_TYPES * r + TYPE_3;
       setstate((char *)cur);
+      pthread_mutex_unlock(&mu);
       return;
     }
     setstate((char *)cur);
   }
+  pthread_mutex_unlock(&mu);
+#endif
   for (long long i = 0; i < n; i++) out[i] = p_drand48();
 }
 

@@ -1765,17 +1765,36 @@ extern "C" int spb_support_from_blur_noalloc(long long n, const float *blur, int
   int *diflags = reinterpret_cast<int *>(s + kNaIntFlags);
   uint8_t *dflags = s + kNaFlags;
   const cudaStream_t st = 0;  // legacy default stream: no stream object is created
-  CK(cudaMemcpyAsync(dblur, blur, sizeof(float2) * (size_t)n, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(diflags, flags, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st));
+  // Every failure after the first enqueue waits for the work already queued,
+  // so that no copy still reads or writes the caller's buffers (or the shared
+  // scratch) once the call has returned.
+  int rc = 0;
+#define NA_CK(call)                                                      \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) {                                             \
+      rc = fail("%s: %s", #call, cudaGetErrorString(e_));                \
+      goto drain;                                                        \
+    }                                                                    \
+  } while (0)
+  NA_CK(cudaMemcpyAsync(dblur, blur, sizeof(float2) * (size_t)n, cudaMemcpyHostToDevice, st));
+  NA_CK(cudaMemcpyAsync(diflags, flags, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st));
   flags_to_u8_kernel<<<148, 256, 0, st>>>(diflags, dflags, n);
   abs_kernel<<<148, 256, 0, st>>>(dblur, dabs, n);
-  CK(cudaGetLastError());
-  if (select_and_mask_on(st, sel, dabs, n, 1, type, value, dflags)) return -1;
+  NA_CK(cudaGetLastError());
+  if (select_and_mask_on(st, sel, dabs, n, 1, type, value, dflags)) {
+    rc = -1;
+    goto drain;
+  }
   flags_to_int_kernel<<<148, 256, 0, st>>>(dflags, diflags, n);
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(flags, diflags, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  NA_CK(cudaGetLastError());
+  NA_CK(cudaMemcpyAsync(flags, diflags, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
+  NA_CK(cudaStreamSynchronize(st));
   return 0;
+#undef NA_CK
+drain:
+  cudaStreamSynchronize(st);  // the error text of the first failure is kept
+  return rc;
 }
 
 // ------------------------------------------------------------------ PRTF

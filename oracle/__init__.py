@@ -44,10 +44,27 @@ _ip = C.POINTER(C.c_int)
 _vp = C.c_void_p
 
 
+def reference_root():
+    """Root of the reference's source tree: ``$SPIMAGE_REFERENCE`` when set,
+    else the ``REF`` default of ``oracle/Makefile``; None when that directory
+    has no ``src/`` (the reference is not present on this machine)."""
+    root = os.environ.get("SPIMAGE_REFERENCE")
+    if not root:
+        with open(os.path.join(HERE, "Makefile")) as f:
+            for line in f:
+                if line.startswith("REF ?="):
+                    root = line.split("?=", 1)[1].strip()
+                    break
+    return root if root and os.path.isdir(os.path.join(root, "src")) else None
+
+
 def build(ref: bool = False) -> None:
     """Compile the restatement (and the reference build when ``ref``)."""
     target = ["all", "ref"] if ref else ["all"]
-    subprocess.run(["make", "-s", "-C", HERE] + target, check=True)
+    extra = []
+    if ref and os.environ.get("SPIMAGE_REFERENCE"):
+        extra = [f"REF={os.environ['SPIMAGE_REFERENCE']}"]
+    subprocess.run(["make", "-s", "-C", HERE] + target + extra, check=True)
 
 
 def ref_available() -> bool:

@@ -118,9 +118,12 @@ def _probe(include_dirs, defines=()):
 
 
 def test_struct_layouts_match_reference_headers():
-    ref_inc = "/root/reference/include"
-    if not os.path.isdir(ref_inc):
+    import oracle
+
+    root = oracle.reference_root()
+    if root is None:
         pytest.skip("reference headers not present")
+    ref_inc = os.path.join(root, "include")
     ours = _probe([os.path.join(ROOT, "include")])
     theirs = _probe([ref_inc, os.path.join(ref_inc, "spimage"), os.path.join(ROOT, "oracle", "stubs"),
                      os.path.join(ROOT, "oracle", "fftw_shim")], ["-D_SP_SINGLE_PRECISION"])

@@ -12,7 +12,7 @@ from tests._engines import AREA, DIFFMAP, ER, HIO, RAAR, RANDOM_PHASES, THRESHOL
 pytestmark = pytest.mark.gpu
 
 RANDOM_VALUES = 4
-MASKED_OUT_ZEROED = 8
+MASKED_OUT_ZEROED = 256  # SpModelMaskedOutZeroed, include/spimage/phasing.h
 
 
 def batch_setup(lib, shape, alg, sup, seeds, constraints=2, beta=0.9, init_flags=RANDOM_PHASES, patterson=None):

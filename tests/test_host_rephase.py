@@ -60,3 +60,39 @@ def test_rephase_matches_per_pixel_draws(env, shape, seed, skip):
     exp, exp_after = _expected(libc, libm, amp, seed, skip)
     assert np.array_equal(got.view(np.uint32), exp.view(np.uint32))
     assert after == exp_after
+
+
+def test_concurrent_rephase_keeps_the_generator(env):
+    """Host threads rephasing at once (ctypes releases the GIL during the
+    call) must not leave the C library's generator on the bulk draw's
+    stand-in state: afterwards sp_srand(s) gives glibc's own sequence."""
+    import threading
+
+    L, so, libc, libm = env
+    libc.srand(123)
+    want = [libc.rand() for _ in range(64)]
+    # many short calls from eight threads: the swaps of the generator state
+    # overlap thousands of times (without the lock this lost the generator
+    # on every run)
+    imgs = [L.new_image((np.random.default_rng(k).random((32, 32))).astype(np.complex64)) for k in range(8)]
+    errors = []
+
+    def work(img):
+        try:
+            for _ in range(20000):
+                so.sp_image_rephase(C.cast(img, C.c_void_p), SP_RANDOM_PHASE)
+        except Exception as e:  # pragma: no cover
+            errors.append(e)
+
+    try:
+        th = [threading.Thread(target=work, args=(im,)) for im in imgs]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+    finally:
+        for im in imgs:
+            L.free_image(im)
+    assert not errors
+    so.sp_srand(123)
+    assert [libc.rand() for _ in range(64)] == want

@@ -257,3 +257,41 @@ def test_restatement_equals_reference_close_centre_template(oracle_mod, name, sh
     assert np.array_equal(res.support(), ref.support())
     assert not np.array_equal(res.support(), (np.real(s0) != 0).astype(np.int32)), "support never changed"
     assert same_bits(res.model(), ref.model())
+
+
+def _margin_or_phased_run(eng, shape, mode):
+    """Amplitude margins (SpAmplitudeErrorMargin, src/phasing.c:1070-1100) or
+    amplitude recovery from phased amplitudes (SpRecoverAmplitudes,
+    src/phasing.c:1103-1109) on one engine."""
+    from libspimage_b200 import synth
+
+    amp, mask, support, obj = synth.small_pattern(shape, seed=2)
+    rng = np.random.default_rng(5)
+    eng.set_algorithm(HIO, beta=0.9, constraints=2 | (32 if mode == "margins" else 0))
+    eng.add_support_update(AREA, 7, 2.0, 0.1)
+    if hasattr(eng, "start"):
+        eng.start()
+    eng.set_amplitudes(amp, mask)
+    if mode == "margins":
+        eng.set_amplitudes_margins((amp * (1 - 0.2 * rng.random(shape))).astype(np.float32),
+                                   (amp * (1 + 0.2 * rng.random(shape))).astype(np.float32))
+    assert eng.init_model(1, seed=4) == 0
+    if mode == "phased":
+        pa = (np.fft.fftn(obj) * np.exp(2j * np.pi * 0.05 * rng.standard_normal(shape))).astype(np.complex64)
+        eng.set_phased_amplitudes(pa, (rng.random(shape) < 0.7).astype(np.int32))
+        eng.set_objective(1)
+    eng.set_support(support)
+    assert eng.iterate(25) == 0
+    return eng
+
+
+@pytest.mark.parametrize("mode", ["margins", "phased"])
+@pytest.mark.parametrize("shape", [(32, 40), (8, 12, 10)])
+def test_margins_and_phased_amplitudes_match_reference(oracle_mod, mode, shape):
+    if not oracle_mod.ref_available():
+        pytest.skip("reference engine not built here")
+    a = _margin_or_phased_run(oracle_mod.Restatement(shape), shape, mode)
+    b = _margin_or_phased_run(oracle_mod.Reference(shape), shape, mode)
+    for w in (0, 1, 2):
+        assert same_bits(a.get(w), b.get(w)), w
+    assert np.array_equal(a.flags(), b.flags())

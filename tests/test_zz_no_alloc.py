@@ -66,3 +66,32 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(lib):
                                           flags.ctypes.data_as(C.POINTER(C.c_int)))
     assert rc == -1
     assert "65536-pixel limit" in so.spb_error_string().decode()
+
+
+def _device_free_bytes():
+    """Free device memory as the driver reports it (cuMemGetInfo on the
+    context the library's calls made current on this thread)."""
+    cu = C.CDLL("libcuda.so.1")
+    free, total = C.c_size_t(), C.c_size_t()
+    rc = cu.cuMemGetInfo_v2(C.byref(free), C.byref(total))
+    assert rc == 0, f"cuMemGetInfo_v2 returned {rc}"
+    return free.value
+
+
+def test_noalloc_leaves_device_memory_unchanged(lib):
+    """The property the entry point exists for: once its kernels are loaded
+    and the scratch address is known (a first call of each case), further
+    calls of interleaved sizes and kinds take no device memory."""
+    so = _entry_points(lib)
+    cases = [_case(4, (256, 256), AREA, 0.05), _case(5, (17, 31), THRESHOLD, 0.4), _case(6, (128, 200), AREA, 0.2)]
+    for c in cases:
+        _run(so, "spb_support_from_blur_noalloc", *c)
+    before = _device_free_bytes()
+    outs = {}
+    for rep in range(3):
+        for k in (2, 0, 1, 0, 2):
+            got = _run(so, "spb_support_from_blur_noalloc", *cases[k])
+            if k in outs:
+                assert np.array_equal(got, outs[k])
+            outs[k] = got
+    assert _device_free_bytes() == before
