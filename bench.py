@@ -266,17 +266,19 @@ def gpu_arm(args):
     if args.batch_steps > 0:
         batched = batched_run(args, L, torch, world)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
-            batched["cpu_baseline"] = cpu_baseline(WORKLOADS["batch512"], args.cpu_sample_slots)
-            batched["cpu_baseline"]["note"] = ("the reference runs random starts one after another "
-                                               "(Reconstructor.reconstruct_loop), so its start-iterations/s "
-                                               "equal its iterations/s")
+            batched["cpu_baseline"] = cpu_baseline(WORKLOADS["batch512"], args.cpu_sample_slots,
+                                                   wl_name="batch512", use="ii")
+            batched["cpu_baseline"]["note"] = ("independent starts on the host: one single-threaded reference "
+                                               "engine per core, each on its own start (mode ii), aggregate "
+                                               "start-iterations/s")
 
     mixed = mixed_run(args, L) if args.mixed_jobs > 0 else None
     serving = serving_run(args, L) if args.serve_window > 0 else None
 
-    cpu = None
+    cpu = fp64 = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(wl, args.cpu_sample_slots)
+        cpu = cpu_baseline(wl, args.cpu_sample_slots, wl_name=args.workload, use="iii")
+        fp64 = error_vs_fp64(args.workload)
 
     if rank == 0:
         line = {
@@ -285,7 +287,7 @@ def gpu_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wl["desc"], "shape": list(wl["shape"]), "slots_per_step": slots,
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before each timed step",
-                       "efourier_final_e2e": efour},
+                       "efourier_final_e2e": efour, "error_vs_fp64": fp64},
             "e2e": {"value": round(e2e_val, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches_total),
             "kernels": {k: {"launches": v[0], "avg_us": round(v[1] / max(v[0], 1) * 1e3, 3)} for k, v in ktimes.items()},
@@ -567,8 +569,11 @@ def serving_run(args, L):
                          "seed": 8 * len(jobs), "period": 20, "pattern": len(jobs)})
         return jobs, arr
 
-    out = {"workload": "Poisson arrivals; 8 starts x (1000 HIO beta 0.9 + 100 ER) per job, area support every 20; "
-                       "sizes 128^2 .30, 256^2 .30, 512^2 .20, 1024^2 .15, 128^3 .05",
+    out = {"workload": f"Poisson arrivals at {args.serve_rate:g}/s for {args.serve_window:g} s (the stated window is 60 s; "
+                       "reduced so that the benchmark run stays within minutes: at this overload the queue, and "
+                       "with it the latency, grows linearly with the window); 8 starts x (1000 HIO beta 0.9 + "
+                       "100 ER) per job, area support every 20; sizes 128^2 .30, 256^2 .30, 512^2 .20, "
+                       "1024^2 .15, 128^3 .05",
            "unit": "jobs/s", "max_active_jobs": args.max_active_jobs}
     with Server(max_active_jobs=args.max_active_jobs, chunk_slots=100) as srv:
         warm, _ = make_jobs(50.0, 0.2, 99)
@@ -696,16 +701,100 @@ def cpu_setup(wl, threads, seed=0):
     return e, kind
 
 
-def cpu_baseline(wl, sample_slots):
-    threads = os.cpu_count() or 1
-    e, kind = cpu_setup(wl, threads)
+def cpu_sample_rate(wl, threads, sample_slots, seed=0):
+    """Iteration slots per second of one CPU engine with `threads` FFT threads
+    over `sample_slots` slots of the workload's first stage."""
+    e, kind = cpu_setup(wl, threads, seed=seed)
     t0 = time.perf_counter()
     e.iterate(sample_slots)
-    dt = time.perf_counter() - t0
-    return {"value": round(sample_slots / dt, 3), "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{sample_slots} iteration slots of the first stage ({wl['stages'][0][0]}, incl. "
-                      f"{sample_slots // wl['period']} support updates) of the same workload; FFT threads = cores, "
-                      "FFTW3 API served by the oracle CPU FFT (no libfftw3f on the box)"}
+    return sample_slots / (time.perf_counter() - t0), kind
+
+
+def cpu_worker(args):
+    """One single-threaded CPU engine of the per-core throughput mode: waits
+    for the common start signal (a line on stdin), times its sample and prints
+    {"slots": ..., "seconds": ...}."""
+    wl = WORKLOADS[args.cpu_worker]
+    e, kind = cpu_setup(wl, 1, seed=args.cpu_worker_seed)
+    sys.stdin.readline()
+    t0 = time.perf_counter()
+    e.iterate(args.cpu_sample_slots)
+    print(json.dumps({"slots": args.cpu_sample_slots, "seconds": time.perf_counter() - t0, "kind": kind}), flush=True)
+
+
+def cpu_per_core(wl_name, procs, sample_slots):
+    """Mode (ii): one independent single-threaded engine per host core (the
+    reference's FFTW planner is not thread-safe, so throughput on many cores
+    means many processes), each on its own start; aggregate slots/s over the
+    slowest process's timed span."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", wl_name, "--cpu-sample-slots", str(sample_slots)]
+    ps = [subprocess.Popen(cmd + ["--cpu-worker-seed", str(k)], stdin=subprocess.PIPE, stdout=subprocess.PIPE,
+                           stderr=subprocess.DEVNULL, text=True) for k in range(procs)]
+    time.sleep(0.5)
+    for p in ps:  # all set up (imports, pattern, start); release them together
+        p.stdin.write("go\n")
+        p.stdin.flush()
+    outs = [json.loads(p.communicate(timeout=600)[0].strip().splitlines()[-1]) for p in ps]
+    slowest = max(o["seconds"] for o in outs)
+    return sum(o["slots"] for o in outs) / slowest, outs[0]["kind"]
+
+
+def cpu_modes(wl_name, sample_slots, per_core_slots):
+    """The reference CPU engine in three modes on this host: (i) one job,
+    one thread (the reference default: sp_init_fft not called); (ii) one
+    single-threaded job per core, aggregate; (iii) one job with
+    sp_init_fft(cores)."""
+    wl = WORKLOADS[wl_name]
+    cores = os.cpu_count() or 1
+    single, kind = cpu_sample_rate(wl, 1, max(1, sample_slots // 4))
+    per_core, _ = cpu_per_core(wl_name, cores, per_core_slots)
+    threaded, _ = cpu_sample_rate(wl, cores, sample_slots)
+    return {"i_single_thread": round(single, 3), "ii_per_core_aggregate": round(per_core, 3),
+            "iii_one_job_all_threads": round(threaded, 3), "cores": cores, "kind": kind,
+            "fft": "FFTW3 API served by the oracle CPU FFT (no libfftw3f on the box)",
+            "samples": f"(i) {max(1, sample_slots // 4)} slots, (ii) {per_core_slots} slots per process x {cores}, "
+                       f"(iii) {sample_slots} slots; first stage ({wl['stages'][0][0]}) of the same workload, "
+                       "support updates included"}
+
+
+def cpu_baseline(wl, sample_slots, wl_name="raar1024", per_core_slots=40, use="iii"):
+    m = cpu_modes(wl_name, sample_slots, per_core_slots)
+    key = {"i": "i_single_thread", "ii": "ii_per_core_aggregate", "iii": "iii_one_job_all_threads"}[use]
+    return {"value": m[key], "unit": UNIT, "cores": m["cores"] if use != "i" else 1, "kind": m["kind"],
+            "mode": key, "modes": m,
+            "sample": m["samples"] + "; " + m["fft"]}
+
+
+def error_vs_fp64(wl_name, iterations=10):
+    """Relative L2 error of the float32 model after `iterations` slots against
+    the FP64 restatement (oracle/fp64.py) from the same start.  The float32
+    engine here is the oracle restatement, whose iterates the GPU library
+    reproduces bit for bit (parity tests), so the figure is the GPU's."""
+    import oracle
+    from oracle.fp64 import Fp64Phaser, rel_l2
+    from libspimage_b200 import synth
+
+    wl = WORKLOADS[wl_name]
+    amp, mask, support, _ = synth.workload(wl["pattern"], seed=0)
+    e = oracle.Restatement(wl["shape"], threads=os.cpu_count() or 1)
+    f = Fp64Phaser(wl["shape"])
+    name, beta, _ = wl["stages"][0]
+    alg = {"HIO": oracle.HIO, "RAAR": oracle.RAAR, "ER": oracle.ER, "DM": oracle.DIFFMAP}[name]
+    for eng in (e, f):
+        eng.set_algorithm(alg, beta=beta, constraints=wl["constraints"])
+        eng.add_support_update(oracle.SUP_AREA, wl["period"], wl["blur"], wl["area"])
+    e.set_amplitudes(amp, mask)
+    e.init_model(oracle.RANDOM_PHASES, seed=0)
+    e.set_support(support)
+    f.set_amplitudes(amp, mask)
+    f.set_flags(e.flags())
+    f.set_model(e.model())
+    e.iterate(iterations)
+    f.iterate(iterations)
+    ef32, ef64 = e.efourier()[0], f.efourier()[0]
+    return {"iterations": iterations, "model_rel_l2": float(f"{rel_l2(e.model(), f.model()):.3e}"),
+            "efourier_rel": float(f"{abs(ef32 - ef64) / ef64:.3e}"),
+            "note": "float32 result (bit-identical on GPU and reference engine) vs FP64 restatement, same start"}
 
 
 def reference_arm(args):
@@ -725,6 +814,7 @@ def reference_arm(args):
         times.append(time.perf_counter() - t0)
     total = float(sum(times))
     value = args.steps * sample / total
+    modes = cpu_modes(args.workload, sample, 40)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3),
@@ -733,7 +823,8 @@ def reference_arm(args):
                    "step": f"bounded sample: {sample} iteration slots of the first stage per step"},
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"{sample} iteration slots per step, FFT threads = cores, FFTW3 API served by "
-                                   "the oracle CPU FFT (no libfftw3f on the box)"},
+                                   "the oracle CPU FFT (no libfftw3f on the box)",
+                         "mode": "iii_one_job_all_threads", "modes": modes},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -757,9 +848,15 @@ def main():
                     help="server admission limit; mixed batch, start-iterations/s by limit on three boxes: "
                          "4/6/8: 67.9k/69.2k/63.6k; 8/12/16/24: 69.7k/63.1k/64.5k/50.9k; 16/32/64/96: 59.5k/56.5k/45.2k/50.3k")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="offered arrivals per second")
-    ap.add_argument("--serve-window", type=float, default=1.0, help="seconds of arrivals (0: skip serving)")
+    ap.add_argument("--serve-window", type=float, default=3.0,
+                    help="seconds of arrivals at --serve-rate (0: skip serving); the stated window is 60 s")
     ap.add_argument("--serve-sustained-window", type=float, default=5.0)
+    ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-worker-seed", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.cpu_worker:
+        cpu_worker(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
