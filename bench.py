@@ -771,7 +771,7 @@ def error_vs_fp64(wl_name, iterations=10):
     engine here is the oracle restatement, whose iterates the GPU library
     reproduces bit for bit (parity tests), so the figure is the GPU's."""
     import oracle
-    from oracle.fp64 import Fp64Phaser, rel_l2
+    from oracle.fp64 import Fp64Phaser, efourier64, rel_l2
     from libspimage_b200 import synth
 
     wl = WORKLOADS[wl_name]
@@ -791,10 +791,11 @@ def error_vs_fp64(wl_name, iterations=10):
     f.set_model(e.model())
     e.iterate(iterations)
     f.iterate(iterations)
-    ef32, ef64 = e.efourier()[0], f.efourier()[0]
+    ef32, ef64 = efourier64(e.model(), amp, e.flags())[0], f.efourier()[0]
     return {"iterations": iterations, "model_rel_l2": float(f"{rel_l2(e.model(), f.model()):.3e}"),
             "efourier_rel": float(f"{abs(ef32 - ef64) / ef64:.3e}"),
-            "note": "float32 result (bit-identical on GPU and reference engine) vs FP64 restatement, same start"}
+            "note": "float32 result (bit-identical on GPU and reference engine) vs FP64 restatement, same start; "
+                    "both Fourier errors summed in float64"}
 
 
 def reference_arm(args):

@@ -245,12 +245,20 @@ class Fp64Phaser:
 
     def efourier(self):
         """(E_F, FcFo) of the model, src/phasing.c:852-891, in float64."""
-        F = np.abs(np.fft.fftn(self.g1))
-        meas = (self.flags_ & MEASURED) != 0
-        A = np.abs(self.amp)
-        nom = ((F - A) ** 2)[meas].sum()
-        den = (A ** 2)[meas].sum() + (F ** 2)[~meas].sum()
-        return float(np.sqrt(nom / den)), float(A[meas].sum() / F[meas].sum())
+        return efourier64(self.g1, self.amp, self.flags_)
+
+
+def efourier64(model, amp, flags):
+    """(E_F, FcFo) of a model (src/phasing.c:852-891) evaluated in float64:
+    for stating the Fourier error of a float32 model without the rounding of
+    the reference's float accumulation."""
+    model = np.asarray(model, np.complex128)
+    F = np.abs(np.fft.fftn(model))
+    meas = (np.asarray(flags).reshape(model.shape) & MEASURED) != 0
+    A = np.abs(np.asarray(amp, np.float64).reshape(model.shape))
+    nom = ((F - A) ** 2)[meas].sum()
+    den = (A ** 2)[meas].sum() + (F ** 2)[~meas].sum()
+    return float(np.sqrt(nom / den)), float(A[meas].sum() / F[meas].sum())
 
 
 def rel_l2(a, b):
