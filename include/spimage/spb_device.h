@@ -81,17 +81,23 @@ const char *spb_kernel_name(int kind);
  * previous iterate: 1 at the start (overlapping the inverse transform), 2
  * between the two transforms (less shared memory, more blocks per SM), 0
  * the built-in choice (2 when the grid exceeds what fits on the device at
- * once with 1).  Setting a knob drops the context's captured graphs. */
-enum { SPB_TUNE_ROW_LINES = 0, SPB_TUNE_NO_PDL = 1, SPB_TUNE_ROW_G0 = 2, SPB_TUNE_KNOBS = 4 };
+ * once with 1); SPB_TUNE_SPLIT = how many points of a line each thread of
+ * the iteration's two passes holds: 1 = 16 (the 16-point kernels), 2 = 8 (the
+ * 8-point kernels, twice the threads per line, for lengths 256, 512, 1024 and
+ * 4096), 0 the built-in choice (8 when the 16-point kernels would give the
+ * SMs fewer than 32 warps of lines).  Setting a knob drops the context's
+ * captured graphs. */
+enum { SPB_TUNE_ROW_LINES = 0, SPB_TUNE_NO_PDL = 1, SPB_TUNE_ROW_G0 = 2, SPB_TUNE_SPLIT = 3, SPB_TUNE_KNOBS = 4 };
 int spb_ctx_set_tuning(spb_ctx *ctx, int knob, int value);
 int spb_ctx_get_tuning(spb_ctx *ctx, int knob);
 /* Autotuner (no reference counterpart): times `calls` calls of `iterations`
  * (2..64) iterations of `alg` for each candidate launch shape (row lines per
- * block, dependent launch on/off) and keeps the fastest; the model, iterates,
- * support and parity are restored afterwards.  The choice is cached per
- * process by (shape, starts, algorithm); force = 1 measures again.  best_ms
- * (optional) receives the chosen time per iteration, -1 when taken from the
- * cache. */
+ * block, dependent launch on/off, where the row pass stages the previous
+ * iterate, 16 or 8 points per thread) and keeps the fastest; the model,
+ * iterates, support and parity are restored afterwards.  The choice is cached
+ * per process by (shape, starts, algorithm); force = 1 measures again.
+ * best_ms (optional) receives the chosen time per iteration, -1 when taken
+ * from the cache. */
 int spb_ctx_autotune(spb_ctx *ctx, const spb_alg_desc *alg, int iterations, int calls, int force, double *best_ms);
 
 /* Host -> device copies of the phaser inputs (src/phasing.c:189-363). */

@@ -255,6 +255,7 @@ PassArgs base_args(const spb_ctx *c) {
   a.row_lpb = c->tune[SPB_TUNE_ROW_LINES];
   a.row_g0 = c->tune[SPB_TUNE_ROW_G0];
   a.pdl = c->tune[SPB_TUNE_NO_PDL] ? 0 : 1;
+  a.split = c->tune[SPB_TUNE_SPLIT];
   a.inv_n = (float)(1.0 / (double)c->n);
   a.nx_f = (float)c->nx;
   a.n_f = (float)c->n;
@@ -1411,13 +1412,13 @@ struct TuneKey {
 };
 std::mutex g_tune_mu;
 struct TuneChoice {
-  int lines, nopdl, g0;
+  int lines, nopdl, g0, split;
 };
 std::map<TuneKey, TuneChoice> g_tune_cache;
 
 int apply_choice(spb_ctx *c, const TuneChoice &t) {
   if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, t.lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, t.nopdl) ||
-      spb_ctx_set_tuning(c, SPB_TUNE_ROW_G0, t.g0))
+      spb_ctx_set_tuning(c, SPB_TUNE_ROW_G0, t.g0) || spb_ctx_set_tuning(c, SPB_TUNE_SPLIT, t.split))
     return -1;
   return 0;
 }
@@ -1448,7 +1449,8 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   }
   const int cur0 = c->cur, xv0 = c->x_valid, xfv0 = c->xf_valid;
   const float xfg0 = c->xf_gamma1;
-  const TuneChoice knob0{c->tune[SPB_TUNE_ROW_LINES], c->tune[SPB_TUNE_NO_PDL], c->tune[SPB_TUNE_ROW_G0]};
+  const TuneChoice knob0{c->tune[SPB_TUNE_ROW_LINES], c->tune[SPB_TUNE_NO_PDL], c->tune[SPB_TUNE_ROW_G0],
+                         c->tune[SPB_TUNE_SPLIT]};
   int rc = 0;
   const float2 *bufs[4] = {c->g[0], c->g[1], c->gp, c->X};
   for (int k = 0; k < 4 && !rc; k++)
@@ -1463,13 +1465,18 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   const int T = c->nx >= 16 ? c->nx / 16 : 1;
   const int lpb_max = 256 / T > 0 ? 256 / T : 1;
   double best = 1e30;
-  TuneChoice bestc{0, 0, 0};
-  for (int cand = 0; cand < 2 * 2 * 16 && !rc; cand++) {
-    const int nopdl = cand & 1, g0 = 1 + ((cand >> 1) & 1), li = cand >> 2;
+  TuneChoice bestc{0, 0, 0, 0};
+  // 8-point kernels exist for these row (x) and projection-axis lengths
+  auto split_len = [](int n) { return n == 256 || n == 512 || n == 1024 || n == 4096; };
+  const bool can_split = split_len(c->nx) || split_len(c->nz > 1 ? c->nz : c->ny);
+  for (int cand = 0; cand < 2 * 2 * 2 * 16 && !rc; cand++) {
+    const int nopdl = cand & 1, g0 = 1 + ((cand >> 1) & 1), sp = 1 + ((cand >> 2) & 1), li = cand >> 3;
     const int lines = li ? 1 << (li - 1) : 0;
     if (lines > lpb_max) continue;  // (0 is the built-in choice, which may be lpb_max or fewer)
+    // the 8-point row kernel has one block shape: no lines-per-block candidates
+    if (sp == 2 && (!can_split || li != 0)) continue;
     {
-      if (apply_choice(c, TuneChoice{lines, nopdl, g0})) {
+      if (apply_choice(c, TuneChoice{lines, nopdl, g0, sp})) {
         rc = -1;
         break;
       }
@@ -1484,7 +1491,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
         rc = fail("autotune: timing failed");
       if (!rc && ms < best) {
         best = ms;
-        bestc = TuneChoice{lines, nopdl, g0};
+        bestc = TuneChoice{lines, nopdl, g0, sp};
       }
     }
   }

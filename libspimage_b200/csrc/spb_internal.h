@@ -73,6 +73,10 @@ struct PassArgs {
   // launch shape: lines per block of the row pass (0: the built-in choice)
   int row_lpb;
   int row_g0;  // g0 staging of the register row pass: 0 auto, 1 at the start, 2 between the transforms
+  // 8 points per thread in the iteration's passes (spb_split.cu): 0 auto
+  // (when the 16-point kernels would leave the SMs short of warps), 1 never,
+  // 2 wherever a kernel exists
+  int split;
   // 1: launch the register pass kernels with programmatic dependent launch
   int pdl;
   // scalars
@@ -109,6 +113,9 @@ struct SelectState {
 // line length or mode has none
 cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
+// 8-point kernels of the iteration's two passes (spb_split.cu)
+cudaError_t launch_row_split(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
+cudaError_t launch_col_split(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_gauss_table(const PassArgs &a, float *tab, cudaStream_t st);
 cudaError_t check_roundings(unsigned lo, unsigned hi, unsigned long long ndiv, unsigned long long seed,
                             unsigned a_stride, unsigned long long *d_bad);

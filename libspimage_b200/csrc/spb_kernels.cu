@@ -283,7 +283,22 @@ static cudaError_t row_launch(const LinePlan &px, const PassArgs &a, cudaStream_
   return row_launch_n<MODE, 0>(px, a, st);
 }
 
+// The 8-point kernels for a pass of `nlines` lines of length n: asked for
+// (knob 2), or chosen when the 16-point kernels' n/16 threads per line would
+// give the SMs fewer than 32 warps (1024 threads) each.
+static bool want_split(const PassArgs &a, int n, long long nlines) {
+  if (a.split == 1) return false;
+  if (a.split == 2) return true;
+  static int nsm = 0;
+  if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) nsm = 148;
+  return nlines * (n / 16) < 1024LL * nsm;
+}
+
 cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st) {
+  if (mode == ROW_ITER && px.n > 0 && want_split(a, px.n, a.n / px.n)) {
+    const cudaError_t se = launch_row_split(mode, px, a, st);
+    if (se != cudaErrorNotSupported) return se;
+  }
   const cudaError_t fe = launch_row_fast(mode, px, a, st);
   if (fe != cudaErrorNotSupported) return fe;
   switch (mode) {
@@ -337,6 +352,11 @@ static cudaError_t col_launch(const LinePlan &pl, const PassArgs &a, cudaStream_
 }
 
 cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArgs &a, cudaStream_t st) {
+  if ((mode == COL_PROJECT || mode == COL_PROJECT_NOFC) && pl.n > 0 &&
+      want_split(a, pl.n, (long long)a.ncols * a.nouter)) {
+    const cudaError_t se = launch_col_split(mode, pl, a, st);
+    if (se != cudaErrorNotSupported) return se;
+  }
   (void)line_len;
   const cudaError_t fe = launch_col_fast(mode, pl, a, st);
   if (fe != cudaErrorNotSupported) return fe;

@@ -85,7 +85,7 @@ def test_raar_1024_then_er_bit_exact(lib, oracle_mod):
     pat = synth.workload("raar1024")
     sup = [(AREA, 50, {0: 3.0, 5000: 0.7}, 0.05)]
     ref = setup_pattern(oracle_mod.Restatement((1024, 1024), threads=8), pat, RAAR, 0.87, sup)
-    gpu = setup_pattern(lib.Phaser((1024, 1024)), pat, RAAR, 0.87, sup)
+    gpu = setup_pattern(lib.Phaser((1024, 1024)), pat, RAAR, 0.87, sup)  # 8 points per thread (built-in choice)
     assert same_bits(gpu.model(), ref.model()), "initial model"
     for n in (120, 81):
         assert ref.iterate(n) == 0 and gpu.iterate(n) == 0
@@ -97,31 +97,59 @@ def test_raar_1024_then_er_bit_exact(lib, oracle_mod):
     assert gpu.iteration == ref.iteration == 221
     assert_same_state(gpu, ref)
     _check_efourier(gpu, ref, oracle_mod)
+    # the same run through the 16-point kernels
+    other = setup_pattern(lib.Phaser((1024, 1024)), pat, RAAR, 0.87, sup)
+    other.set_tuning(SPLIT, 1)
+    for n in (120, 81):
+        assert other.iterate(n) == 0
+    other.set_algorithm(ER, constraints=2)
+    assert other.iterate(20) == 0
+    assert same_bits(other.model(), ref.model())
 
 
-def test_hio_512_batch_g0_late_bit_exact(lib, oracle_mod):
+SPLIT, ROW_G0 = 3, 2  # tuning knobs: points per thread (1: 16, 2: 8), g0 staging (1: early, 2: late)
+
+
+@pytest.mark.parametrize("split,g0", [(1, 0), (1, 1), (2, 1), (2, 2)])
+def test_hio_512_batch_bit_exact(lib, oracle_mod, split, g0):
     """Eight starts of the batched 512x512 workload (128 blob, 1e7 photons,
-    beamstop 6), HIO beta 0.9 with area support every 20.  The batch's row
-    pass grid is 64 blocks per start (512 rows, 8 rows per block), 512 blocks
-    in all, more than the 3 blocks per SM x 148 SMs that fit with the
-    previous iterate staged up front, so the launcher stages it between the
-    two transforms (the form the 512-start benchmark runs).  Starts 0 and 7
-    are compared with oracle runs of seeds 0 and 7."""
+    beamstop 6), HIO beta 0.9 with area support every 20, on every form of
+    the iteration's passes: 16 points per thread with the previous iterate
+    staged as the launcher chooses (the row grid is 64 blocks per start, 512
+    in all, more than the 3 blocks per SM x 148 SMs that fit with the early
+    staging, so it stages between the transforms: the form of the 512-start
+    benchmark) or up front, and 8 points per thread with either staging.
+    Starts 0 and 7 are compared with oracle runs of seeds 0 and 7."""
     pat = synth.workload("batch512")
     sup = [(AREA, 20, {0: 3.0, 2200: 0.7}, 0.05)]
     seeds = list(range(8))
     gpu = setup_pattern(lib.Phaser((512, 512)), pat, HIO, 0.9, sup, starts=seeds)
+    gpu.set_tuning(SPLIT, split)
+    gpu.set_tuning(ROW_G0, g0)
     assert gpu.iterate(61) == 0
     for s in (0, 7):
         ref = setup_pattern(oracle_mod.Restatement((512, 512), threads=8), pat, HIO, 0.9, sup, seed=s)
         assert ref.iterate(61) == 0
         assert_same_state(gpu, ref, start=s)
-    # the same batch with the early staging forced: same bits
-    early = setup_pattern(lib.Phaser((512, 512)), pat, HIO, 0.9, sup, starts=seeds)
-    early.set_tuning(2, 1)
-    assert early.iterate(61) == 0
-    for s in (0, 7):
-        assert same_bits(early.start_model(s), gpu.start_model(s))
+
+
+@pytest.mark.parametrize("split", [1, 2])
+@pytest.mark.parametrize("shape,alg", [((256, 256), HIO), ((512, 512), RAAR), ((256, 256), DIFFMAP),
+                                       ((1024, 256), ER), ((256, 1024), HIO)])
+def test_single_pattern_points_per_thread_bit_exact(lib, oracle_mod, split, shape, alg):
+    """One pattern through the 16-point (split 1) and 8-point (split 2)
+    kernels of the iteration's passes against the oracle: the 8-point row
+    pass runs for rows of 256/512/1024 points, the 8-point projection pass
+    for columns of those lengths (difference map: both projections)."""
+    pat = synth.make_pattern(shape, min(shape) // 4, 1e7, min(shape) / 64.0, seed=3)
+    sup = [(AREA, 9, {0: 3.0, 60: 0.7}, 0.05)]
+    ref = setup_pattern(oracle_mod.Restatement(shape, threads=8), pat, alg, 0.87, sup, seed=2)
+    gpu = setup_pattern(lib.Phaser(shape), pat, alg, 0.87, sup, seed=2)
+    gpu.set_tuning(SPLIT, split)
+    for n in (23, 70):
+        assert ref.iterate(n) == 0 and gpu.iterate(n) == 0
+        assert same_bits(gpu.model(), ref.model()), f"after {gpu.iteration} slots"
+    assert_same_state(gpu, ref)
 
 
 def test_vol128_hio_one_support_update_bit_exact(lib, oracle_mod):
