@@ -106,13 +106,17 @@ __device__ __forceinline__ void bf16_half(float2 (&a)[8], bool h) {
   a[2] = sel(h, mul_w8_1<INV>(a[2]), a[2]);
   a[4] = sel(h, mul_w4<INV>(a[4]), a[4]);
   a[6] = sel(h, mul_w8_3<INV>(a[6]), a[6]);
-  // second layer: DFT4 over q2 for k1 = 2h + f; (e, k1) sits in register e + 2*k1
+  // second layer: DFT4 over q2 for k1 = 2h + f; (e, k1) sits in register
+  // e + 2*k1 of b (the outputs overwrite a)
+  float2 b[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) b[i] = a[i];
 #pragma unroll
   for (int f = 0; f < 2; f++) {
     float2 in[4];
 #pragma unroll
     for (int e = 0; e < 2; e++) {
-      const float2 lo = a[e + 2 * f], hi = a[e + 4 + 2 * f];  // k1 = f, k1 = 2 + f
+      const float2 lo = b[e + 2 * f], hi = b[e + 4 + 2 * f];  // k1 = f, k1 = 2 + f
       const float2 r = shfl16(sel(h, lo, hi));                 // the partner's q2 = 2(1-h) + e at my k1
       in[e] = sel(h, r, lo);
       in[2 + e] = sel(h, hi, r);
@@ -301,7 +305,7 @@ __device__ __forceinline__ void project8(float2 (&v)[8], const float *amp_l, con
 // kernel: [twiddles N][LPB exchange lines][LPB rows of g0 unless G0LATE]
 // [LPB rows of flags].
 template <int N, bool G0LATE>
-__global__ void __launch_bounds__(256) row_split_kernel(PassArgs a, const float2 *__restrict__ stw, int nrows) {
+__global__ void __launch_bounds__(512) row_split_kernel(PassArgs a, const float2 *__restrict__ stw, int nrows) {
   constexpr int T = N / 16;
   constexpr int TL = 2 * T;  // threads per line
   constexpr int S = N + N / 16;
