@@ -193,7 +193,7 @@ __device__ __forceinline__ void project16(float2 (&v)[16], const float *amp_l, c
     for (int q = 0; q < 16; q++) {
       const float amp = amp_l[t + T * q];
       const float m = div_rn_nb(amp, sqrt_rn_nb(s2[q]));
-      const float2 p = isfinite(m) ? __fmul2_rn(v[q], make_float2(m, m)) : make_float2(amp, 0.0f);
+      const float2 p = isfinite(m) ? make_float2(fmul(v[q].x, m), fmul(v[q].y, m)) : make_float2(amp, 0.0f);
       if ((mm >> q) & 1u) v[q] = p;
     }
   } else {

@@ -33,18 +33,14 @@ __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b)
 // Complex add and subtract as one packed f32x2 add (sm_100): each lane is
 // rounded exactly as __fadd_rn, and a - b is a + (-b) by IEEE definition, so
 // the bits equal the scalar recipe's while the instruction count halves.
+// Multiplies stay scalar: a packed product feeding a packed add is not kept
+// apart from it (measured: one-ulp differences), a scalar __fmul_rn is.
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
-// (a.re*w.re - a.im*w.im, a.re*w.im + a.im*w.re), each product rounded:
-// two packed products (a.re*w.re, a.re*w.im) and (a.im*(-w.im), a.im*w.re)
-// and one packed add.  Round-to-nearest is symmetric, so a.im*(-w.im) is
-// exactly -(a.im*w.im), and t1 + (-t2) is t1 - t2 by IEEE definition: the
-// bits of the scalar recipe t1 = a.re*w.re, t2 = a.im*w.im, t3 = a.re*w.im,
-// t4 = a.im*w.re, (t1 - t2, t3 + t4), in three instructions instead of six.
+// (a.re*w.re - a.im*w.im, a.re*w.im + a.im*w.re), each product rounded
 __device__ __forceinline__ float2 cmulw(float2 a, float wr, float wi) {
-  const float2 p = __fmul2_rn(make_float2(a.x, a.x), make_float2(wr, wi));
-  const float2 q = __fmul2_rn(make_float2(a.y, a.y), make_float2(-wi, wr));
-  return __fadd2_rn(p, q);
+  const float t1 = fmul(a.x, wr), t2 = fmul(a.y, wi), t3 = fmul(a.x, wi), t4 = fmul(a.y, wr);
+  return make_float2(fsub(t1, t2), fadd(t3, t4));
 }
 // |a| as the reference computes it: sqrt(im*im + re*re) rounded once
 __device__ __forceinline__ float cabs_ref(float2 a) { return __fsqrt_rn(fadd(fmul(a.y, a.y), fmul(a.x, a.x))); }

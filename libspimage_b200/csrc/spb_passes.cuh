@@ -72,7 +72,7 @@ __device__ __forceinline__ float2 project_with(float2 G, float amp, bool measure
     if (av < lo) m = __fdiv_rn(lo, av);
     else if (av > hi) m = __fdiv_rn(hi, av);
   }
-  if (isfinite(m)) return __fmul2_rn(G, make_float2(m, m));
+  if (isfinite(m)) return make_float2(fmul(G.x, m), fmul(G.y, m));
   return make_float2(amp, 0.0f);
 }
 

@@ -7,9 +7,8 @@
 namespace spb {
 
 __device__ __forceinline__ float2 scale_cmul_dev(float2 v, float s) {
-  // sp_image_scale: complex multiply by (s, 0), (x*s - y*0, x*0 + s*y) with
-  // every product rounded -- cmulw's recipe with w = (s, 0)
-  return cmulw(v, s, 0.0f);
+  // sp_image_scale: complex multiply by (s, 0)
+  return make_float2(fsub(fmul(v.x, s), fmul(v.y, 0.0f)), fadd(fmul(v.x, 0.0f), fmul(s, v.y)));
 }
 
 // beta of this iteration: kernel argument, or the device table during graph replays
@@ -109,7 +108,7 @@ __device__ __forceinline__ float2 project_vals(float2 G, uint8_t f, float amp, l
         if (av < lo) m = __fdiv_rn(lo, av);
         else if (av > hi) m = __fdiv_rn(hi, av);
       }
-      if (isfinite(m)) G = __fmul2_rn(G, make_float2(m, m));
+      if (isfinite(m)) G = make_float2(fmul(G.x, m), fmul(G.y, m));
       else G = make_float2(amp, 0.0f);
     }
   } else {

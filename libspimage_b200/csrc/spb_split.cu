@@ -288,7 +288,7 @@ __device__ __forceinline__ void project8(float2 (&v)[8], const float *amp_l, con
     for (int q = 0; q < 8; q++) {
       const float amp = amp_l[t + T * (2 * hh + split::mi0(q))];
       const float m = div_rn_nb(amp, sqrt_rn_nb(s2[q]));
-      const float2 p = isfinite(m) ? __fmul2_rn(v[q], make_float2(m, m)) : make_float2(amp, 0.0f);
+      const float2 p = isfinite(m) ? make_float2(fmul(v[q].x, m), fmul(v[q].y, m)) : make_float2(amp, 0.0f);
       if ((mm >> q) & 1u) v[q] = p;
     }
   } else {
