@@ -285,13 +285,17 @@ static cudaError_t row_launch(const LinePlan &px, const PassArgs &a, cudaStream_
 
 // The 8-point kernels for a pass of `nlines` lines of length n: asked for
 // (knob 2), or chosen when the 16-point kernels' n/16 threads per line would
-// give the SMs fewer than 32 warps (1024 threads) each.
+// give the SMs fewer than 8 warps (256 threads) each.  Measured on one B200,
+// iterations per second of one pattern, 16 -> 8 points per thread: 256x256
+// 80.1k -> 96.9k (0.9 warps per SM with 16 points), 512x512 69.4k -> 72.3k
+// (3.5), 1024x1024 47.8k -> 44.3k (13.8: the extra selects and shuffles
+// outweigh the added warps once the passes are near issue-bound).
 static bool want_split(const PassArgs &a, int n, long long nlines) {
   if (a.split == 1) return false;
   if (a.split == 2) return true;
   static int nsm = 0;
   if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) nsm = 148;
-  return nlines * (n / 16) < 1024LL * nsm;
+  return nlines * (n / 16) < 256LL * nsm;
 }
 
 cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st) {

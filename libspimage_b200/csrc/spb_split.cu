@@ -1,9 +1,10 @@
 // Register-resident pass kernels with 8 points per thread, for patterns whose
 // lines are too few to fill the GPU with the 16-point kernels of spb_fast.cu
-// (a single 1024x1024 pattern has 1024 lines per pass: 64 threads a line at
-// 16 points each give 13-14 warps per SM, and the passes wait on latency).
-// Here a line of N points is held by 2T threads (T = N/16 thread pairs), so
-// twice the warps share the same work.
+// (a single 256x256 pattern has 256 lines per pass: 16 threads a line at 16
+// points each give less than one warp per SM, and the passes wait on
+// latency).  Here a line of N points is held by 2T threads (T = N/16 thread
+// pairs), so twice the warps share the same work, for some 20 % more
+// instructions (the selects and shuffles of the split butterflies).
 //
 // The transform is the same one, operation for operation: the canonical
 // radix plan, the butterflies of spb_fft.cuh and the same twiddle values, so
