@@ -18,6 +18,17 @@
  * sp_phaser_init_models_device, sp_phaser_iterate), so its results are bit for
  * bit those of the same schedule run alone.
  *
+ * Failure handling: a job ends early, with a negative status and an error
+ * text, when its work fails on the device (SPB_JOB_FAILED; its context is
+ * freed), when it is cancelled (SPB_JOB_CANCELLED), when a model of one of
+ * its starts holds NaN or infinite values after a chunk (SPB_JOB_NONFINITE:
+ * every chunk is followed by a check on the job's stream), or when its
+ * wall-clock budget since submission runs out (SPB_JOB_EXPIRED).  Running
+ * jobs stop at their next chunk boundary, after the chunks already on the
+ * GPU; the server and the other jobs carry on.  The reference's phaser
+ * returns negative codes for its own errors (src/phasing.c:898-998) and
+ * exits on CUDA errors; here no job's failure ends the process.
+ *
  * Return values: 0 success, negative error; the error text of a call is
  * spb_server_last_error(), that of a failed job spb_server_job_error().
  */
@@ -60,10 +71,22 @@ typedef struct {
   float blur_start, blur_end; /* blur radius, Bezier from the first to the last slot */
   unsigned long long seed; /* start b gets random phases keyed by seed + b (device Philox4x32-10) */
   int keep_models;        /* 1: keep every start's final model for spb_server_result */
+  double time_budget_s;   /* wall-clock seconds from submission after which the job ends as
+                             SPB_JOB_EXPIRED; 0: no limit */
 } spb_job;
 
+/* spb_job_info.status */
+enum {
+  SPB_JOB_DONE = 0,
+  SPB_JOB_RUNNING = 1,     /* pending or running */
+  SPB_JOB_FAILED = -1,     /* device or set-up error */
+  SPB_JOB_CANCELLED = -2,  /* spb_server_cancel */
+  SPB_JOB_NONFINITE = -3,  /* NaN or infinity in a model */
+  SPB_JOB_EXPIRED = -4     /* time_budget_s ran out */
+};
+
 typedef struct {
-  int status;    /* 0 done, 1 pending or running, negative: failed */
+  int status;    /* SPB_JOB_DONE, SPB_JOB_RUNNING or a negative SPB_JOB_* code */
   int starts;
   long long slots; /* iteration slots per start */
   double t_submit, t_admit, t_finish; /* seconds since the server was created; -1 if not reached */
@@ -77,6 +100,10 @@ long long spb_server_submit(spb_server *srv, const spb_job *job);
 /* waits until the job has finished or timeout_s has passed (timeout_s < 0:
  * no limit); info->status tells which; returns -1 for an unknown id */
 int spb_server_wait(spb_server *srv, long long id, double timeout_s, spb_job_info *info);
+/* Cancels a job: a pending job ends at once, a running one at its next
+ * chunk boundary (its context stays reusable).  Returns -1 for an unknown id
+ * or a job that has already ended. */
+int spb_server_cancel(spb_server *srv, long long id);
 /* results of a finished job: final Fourier error and support fraction of
  * every start ([starts] each) and, if the job kept them, the models
  * ([starts][N] complex, interleaved re/im); NULL skips an output.  Releases

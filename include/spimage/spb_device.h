@@ -145,6 +145,14 @@ int spb_ctx_get_image(spb_ctx *ctx, int which, float *out);
 int spb_ctx_efourier_sums(spb_ctx *ctx, double sums[4]);
 int spb_ctx_ereal_sums(spb_ctx *ctx, double sums[2]);
 int spb_ctx_support_count(spb_ctx *ctx, long long *count);
+/* No reference counterpart.  Enqueues on the context's stream a check of
+ * every start's current model for NaN or infinite values and a copy of the
+ * result to *host_flag (page-locked host memory): 1 if such a value was
+ * found by this or an earlier check since the last reset, else 0, readable
+ * once the stream has passed this point.  reset = 1 clears the sticky device
+ * flag first.  The reconstruction server runs it after every chunk of a job
+ * to fail a job whose iterates diverged. */
+int spb_ctx_nonfinite_async(spb_ctx *ctx, int reset, unsigned *host_flag);
 
 /* Batched starts.  A batch context holds nb independent reconstructions of
  * ONE pattern (shared amplitudes, margins and measured mask; per-start model,

@@ -43,6 +43,7 @@ struct Slot {
   bool busy = false;
   double last_used = 0;
   Image *amp_img = nullptr, *sup_img = nullptr, *model_img = nullptr;
+  unsigned *nf_host = nullptr;  // page-locked: the job's sticky non-finite flag after its last checked chunk
 };
 
 struct Job {
@@ -63,6 +64,8 @@ struct Job {
   int stage = 0, stage_left = 0;
   long long issued = 0;
   std::deque<cudaEvent_t> inflight;
+  std::deque<long long> inflight_slots;  // slots done when the matching event completes
+  bool cancel = false;                   // set by spb_server_cancel (under mu)
   // results
   std::vector<float> efourier, sfrac, models;
 };
@@ -115,6 +118,7 @@ void destroy_slot_objects(Slot &s) {
   if (s.amp_img) sp_image_free(s.amp_img);
   if (s.sup_img) sp_image_free(s.sup_img);
   if (s.model_img) sp_image_free(s.model_img);
+  if (s.nf_host) cudaFreeHost(s.nf_host);
   s = Slot();
 }
 
@@ -183,6 +187,13 @@ Slot *spb_server::acquire_slot(const spb_job &d, long long need, bool *no_room) 
   }
   s.amp_img = sp_image_alloc(d.nx, d.ny, d.nz);
   s.sup_img = sp_image_alloc(d.nx, d.ny, d.nz);
+  if (cudaMallocHost(&s.nf_host, sizeof(unsigned)) != cudaSuccess) {
+    s.nf_host = nullptr;
+    fail("context set-up: cudaMallocHost failed");
+    free_slot(&s);
+    return nullptr;
+  }
+  *s.nf_host = 0;
   std::lock_guard<std::mutex> lk(mu);
   stats[4] += 1;
   if ((double)held_bytes > stats[3]) stats[3] = (double)held_bytes;
@@ -225,6 +236,7 @@ void spb_server::release_job_objects(Job &j) {
   }
   for (cudaEvent_t e : j.inflight) free_events.push_back(e);
   j.inflight.clear();
+  j.inflight_slots.clear();
 }
 
 int spb_server::start_job(Job &j) {
@@ -299,10 +311,14 @@ int spb_server::issue_chunk(Job &j) {
   const int rc = sp_phaser_iterate(ph, k);
   if (rc) return fail("sp_phaser_iterate returned " + std::to_string(rc) + ": " + sp_phaser_last_error());
   j.stage_left -= k;
+  // every start's model checked for NaN/infinity after the chunk (sticky since the job's first chunk)
+  if (spb_ctx_nonfinite_async((spb_ctx *)sp_phaser_device_context(ph), j.issued == 0 ? 1 : 0, j.slot->nf_host))
+    return fail(std::string("non-finite check: ") + spb_error_string());
   j.issued += k;
   cudaEvent_t e = get_event();
   if (!e || cudaEventRecord(e, j.slot->st) != cudaSuccess) return fail("cudaEventRecord failed");
   j.inflight.push_back(e);
+  j.inflight_slots.push_back(j.issued);
   return 1;
 }
 
@@ -310,12 +326,15 @@ void spb_server::finish_job(const std::shared_ptr<Job> &jp, int status, const st
   Job &j = *jp;
   release_job_objects(j);
   if (j.slot) {
-    if (status == 0) {
+    if (status == SPB_JOB_FAILED) {
+      cudaStreamSynchronize(j.slot->st);
+      free_slot(j.slot);  // its state is unknown after a device or set-up error
+    } else {
+      // done, cancelled, diverged or out of time: the context is sound once
+      // the chunks already queued on its stream have run
+      if (status != 0) cudaStreamSynchronize(j.slot->st);
       j.slot->busy = false;
       j.slot->last_used = now();
-    } else {
-      cudaStreamSynchronize(j.slot->st);
-      free_slot(j.slot);  // its state is unknown after an error
     }
     j.slot = nullptr;
   }
@@ -335,12 +354,29 @@ void spb_server::finish_job(const std::shared_ptr<Job> &jp, int status, const st
 // Admits the first pending job (in arrival order) that fits; false when none
 // could be admitted.
 bool spb_server::admit_one() {
-  if ((int)active.size() >= cfg.max_active_jobs) return false;
   std::vector<std::shared_ptr<Job>> cand;
   {
     std::lock_guard<std::mutex> lk(mu);
     cand.assign(pending.begin(), pending.end());
   }
+  // pending jobs whose time budget ran out end here, whether or not a slot is free
+  for (auto &jp : cand) {
+    Job &j = *jp;
+    if (j.desc.time_budget_s > 0 && now() - j.t_submit > j.desc.time_budget_s) {
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto it = pending.begin(); it != pending.end(); ++it)
+          if (*it == jp) {
+            pending.erase(it);
+            break;
+          }
+      }
+      finish_job(jp, SPB_JOB_EXPIRED, "time budget of " + std::to_string(j.desc.time_budget_s) +
+                                          " s ran out before the job was admitted");
+      return true;
+    }
+  }
+  if ((int)active.size() >= cfg.max_active_jobs) return false;
   for (auto &jp : cand) {
     Job &j = *jp;
     const long long need = spb_ctx_footprint(j.desc.nx, j.desc.ny, j.desc.nz, j.desc.starts, has_dm(j.desc));
@@ -399,18 +435,40 @@ void spb_server::run() {
         const cudaError_t q = cudaEventQuery(j.inflight.front());
         if (q == cudaErrorNotReady) break;
         if (q != cudaSuccess) {
-          err = -1;
+          err = SPB_JOB_FAILED;
           msg = std::string("device error: ") + cudaGetErrorString(q);
           break;
         }
+        const long long done_slots = j.inflight_slots.front();
         free_events.push_back(j.inflight.front());
         j.inflight.pop_front();
+        j.inflight_slots.pop_front();
         progress = true;
+        // the chunk's check has been copied back with it
+        if (*j.slot->nf_host) {
+          err = SPB_JOB_NONFINITE;
+          msg = "a model holds NaN or infinite values after " + std::to_string(done_slots) + " iteration slots";
+          break;
+        }
+      }
+      if (!err) {
+        bool cancel;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          cancel = j.cancel;
+        }
+        if (cancel) {
+          err = SPB_JOB_CANCELLED;
+          msg = "cancelled";
+        } else if (j.desc.time_budget_s > 0 && now() - j.t_submit > j.desc.time_budget_s) {
+          err = SPB_JOB_EXPIRED;
+          msg = "time budget of " + std::to_string(j.desc.time_budget_s) + " s ran out";
+        }
       }
       while (!err && j.issued < j.slots && (int)j.inflight.size() < cfg.chunks_ahead) {
         const int r = issue_chunk(j);
         if (r < 0) {
-          err = -1;
+          err = SPB_JOB_FAILED;
           msg = g_err;
         }
         if (r <= 0) break;
@@ -425,14 +483,14 @@ void spb_server::run() {
         j.sfrac.assign((size_t)nb, 0.0f);
         if (sp_phaser_starts_efourier(ph, j.efourier.data(), nullptr) ||
             sp_phaser_starts_support_fraction(ph, j.sfrac.data())) {
-          err = -1;
+          err = SPB_JOB_FAILED;
           msg = std::string("results: ") + sp_phaser_last_error();
         } else if (j.desc.keep_models) {
           if (!j.slot->model_img) j.slot->model_img = sp_image_alloc(j.desc.nx, j.desc.ny, j.desc.nz);
           j.models.resize(2 * n * (size_t)nb);
           for (int b = 0; b < nb && !err; b++) {
             if (sp_phaser_start_model(ph, b, j.slot->model_img)) {
-              err = -1;
+              err = SPB_JOB_FAILED;
               msg = std::string("model download: ") + sp_phaser_last_error();
             } else {
               memcpy(j.models.data() + 2 * n * (size_t)b, j.slot->model_img->image->data, sizeof(float) * 2 * n);
@@ -552,6 +610,30 @@ extern "C" int spb_server_wait(spb_server *s, long long id, double timeout_s, sp
   if (timeout_s < 0) s->cv_done.wait(lk, done);
   else s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done);
   fill_info(*j, info);
+  return 0;
+}
+
+extern "C" int spb_server_cancel(spb_server *s, long long id) {
+  std::shared_ptr<Job> jp;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return fail("unknown job id " + std::to_string(id));
+    jp = it->second;
+    if (jp->status != SPB_JOB_RUNNING) return fail("job " + std::to_string(id) + " has already ended");
+    for (auto p = s->pending.begin(); p != s->pending.end(); ++p)
+      if (*p == jp) {  // not admitted yet: ends here
+        s->pending.erase(p);
+        jp->status = SPB_JOB_CANCELLED;
+        jp->err = "cancelled";
+        jp->t_finish = s->now();
+        s->stats[7] += 1;
+        s->cv_done.notify_all();
+        return 0;
+      }
+    jp->cancel = true;  // running: the worker ends it at the next chunk boundary
+  }
+  s->cv_work.notify_all();
   return 0;
 }
 

@@ -227,6 +227,7 @@ struct spb_ctx {
   SupportParams spar_shadow{};
   SelectState *sel = nullptr;  // one per start
   double *red = nullptr;       // reduce_scratch_doubles(nb)
+  unsigned *nonfinite = nullptr;  // sticky flag of spb_ctx_nonfinite_async
   unsigned long long *seeds = nullptr;  // per-start generator keys (device starts)
   int x_valid = 0, xf_valid = 0;
   float xf_gamma1 = 0.0f;
@@ -491,6 +492,7 @@ extern "C" int spb_ctx_create_batch(spb_ctx **out, int nx, int ny, int nz, int n
   alloc((void **)&c->gtab, sizeof(float) * (size_t)gauss_table_len(nx, ny, nz));
   alloc((void **)&c->sel, sizeof(SelectState) * (size_t)nb);
   alloc((void **)&c->red, sizeof(double) * (size_t)reduce_scratch_doubles(nb));
+  alloc((void **)&c->nonfinite, sizeof(unsigned));
   alloc((void **)&c->seeds, sizeof(unsigned long long) * (size_t)nb);
   alloc((void **)&c->beta_zero, sizeof(int));
   alloc((void **)&c->spar, sizeof(SupportParams));
@@ -581,6 +583,7 @@ extern "C" long long spb_ctx_footprint(int nx, int ny, int nz, int nb, int dm) {
   b += 4 * gauss_table_len(nx, ny, nz);         // gtab
   b += (long long)sizeof(SelectState) * nb;     // sel
   b += 8LL * reduce_scratch_doubles(nb);        // red
+  b += 256;                                     // non-finite flag (one allocation)
   b += 8LL * nb + 4 + 4LL * kBetaCap;           // seeds, beta_base, beta table
   b += 4 * n + n / 8 + 4096;                    // amp_line, meas_bits (upper bound)
   b += 8LL * 2 * (nx + ny + nz) + 8LL * 3 * 65536;  // twiddles and stage tables (upper bound)
@@ -592,7 +595,7 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
-                  c->gp, c->T, c->absb, c->gtab, c->sel, c->red, c->ax.tw, c->ay.tw, c->az.tw,
+                  c->gp, c->T, c->absb, c->gtab, c->sel, c->red, c->nonfinite, c->ax.tw, c->ay.tw, c->az.tw,
                   c->amp_line, c->amp_bad, c->meas_bits, c->beta_dev, c->beta_base, c->seeds, c->beta_zero, c->spar};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1584,6 +1587,30 @@ extern "C" int spb_ctx_ereal_sums(spb_ctx *c, double sums[2]) {
   if (spb_ctx_batch_ereal_sums(c, h.data())) return -1;
   sums[0] = h[0];
   sums[1] = h[1];
+  return 0;
+}
+
+namespace spb {
+// ORs 1 into *flag when any of the n complex values is NaN or infinite
+__global__ void nonfinite_kernel(const float2 *__restrict__ g, long long n, unsigned *flag) {
+  unsigned bad = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 v = g[i];
+    bad |= (isfinite(v.x) && isfinite(v.y)) ? 0u : 1u;
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+}  // namespace spb
+
+extern "C" int spb_ctx_nonfinite_async(spb_ctx *c, int reset, unsigned *host_flag) {
+  if (!host_flag) return fail("spb_ctx_nonfinite_async: null flag");
+  if (reset) CK(cudaMemsetAsync(c->nonfinite, 0, sizeof(unsigned), c->st));
+  long long blocks = (c->ntot + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  nonfinite_kernel<<<(unsigned)blocks, 256, 0, c->st>>>(c->g[c->cur], c->ntot, c->nonfinite);
+  CK(cudaGetLastError());
+  c->launches++;
+  CK(cudaMemcpyAsync(host_flag, c->nonfinite, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
   return 0;
 }
 

@@ -31,7 +31,11 @@ class Job(C.Structure):
                 ("amplitudes", C.POINTER(C.c_float)), ("mask", C.POINTER(C.c_int)), ("support", C.POINTER(C.c_int)),
                 ("constraints", C.c_int), ("nstages", C.c_int), ("stage", JobStage * MAX_STAGES),
                 ("support_period", C.c_int), ("support_area", C.c_float), ("blur_start", C.c_float),
-                ("blur_end", C.c_float), ("seed", C.c_ulonglong), ("keep_models", C.c_int)]
+                ("blur_end", C.c_float), ("seed", C.c_ulonglong), ("keep_models", C.c_int),
+                ("time_budget_s", C.c_double)]
+
+# spb_job_info.status (include/spimage/serve.h)
+JOB_DONE, JOB_RUNNING, JOB_FAILED, JOB_CANCELLED, JOB_NONFINITE, JOB_EXPIRED = 0, 1, -1, -2, -3, -4
 
 
 class JobInfo(C.Structure):
@@ -48,6 +52,7 @@ def _bind(lib):
         "spb_server_destroy": (None, [vp]),
         "spb_server_submit": (C.c_longlong, [vp, C.POINTER(Job)]),
         "spb_server_wait": (C.c_int, [vp, C.c_longlong, C.c_double, C.POINTER(JobInfo)]),
+        "spb_server_cancel": (C.c_int, [vp, C.c_longlong]),
         "spb_server_result": (C.c_int, [vp, C.c_longlong, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                         C.POINTER(C.c_float)]),
         "spb_server_stats": (C.c_int, [vp, C.POINTER(C.c_double)]),
@@ -101,7 +106,7 @@ class Server:
             pass
 
     def submit(self, amplitudes, mask, support, stages, starts=1, seed=0, constraints=2, support_period=0,
-               area=0.05, blur=(3.0, 0.7), keep_models=False):
+               area=0.05, blur=(3.0, 0.7), keep_models=False, time_budget_s=0.0):
         amp = np.ascontiguousarray(amplitudes, np.float32)
         m = np.ascontiguousarray(mask, np.int32)
         s = np.ascontiguousarray(support, np.int32)
@@ -120,6 +125,7 @@ class Server:
         j.blur_start, j.blur_end = float(blur[0]), float(blur[1])
         j.seed = int(seed)
         j.keep_models = 1 if keep_models else 0
+        j.time_budget_s = float(time_budget_s)
         jid = self.lib.spb_server_submit(self.h, C.byref(j))
         if jid < 0:
             raise RuntimeError(self.lib.spb_server_last_error().decode())
@@ -133,10 +139,16 @@ class Server:
         return {"status": info.status, "starts": info.starts, "slots": info.slots, "t_submit": info.t_submit,
                 "t_admit": info.t_admit, "t_finish": info.t_finish}
 
+    def cancel(self, jid):
+        """Cancels a pending or running job (a running one stops at its next chunk boundary)."""
+        if self.lib.spb_server_cancel(self.h, jid) != 0:
+            raise RuntimeError(self.lib.spb_server_last_error().decode())
+
     def job_error(self, jid):
         return self.lib.spb_server_job_error(self.h, jid).decode()
 
     def result(self, jid):
+        """Results of a finished job (releases it); raises for a job that ended with an error."""
         shape, starts, keep = self._shapes.pop(jid)
         ef = np.zeros(starts, np.float32)
         sf = np.zeros(starts, np.float32)

@@ -85,7 +85,7 @@ def test_raar_1024_then_er_bit_exact(lib, oracle_mod):
     pat = synth.workload("raar1024")
     sup = [(AREA, 50, {0: 3.0, 5000: 0.7}, 0.05)]
     ref = setup_pattern(oracle_mod.Restatement((1024, 1024), threads=8), pat, RAAR, 0.87, sup)
-    gpu = setup_pattern(lib.Phaser((1024, 1024)), pat, RAAR, 0.87, sup)  # 8 points per thread (built-in choice)
+    gpu = setup_pattern(lib.Phaser((1024, 1024)), pat, RAAR, 0.87, sup)  # the built-in choice: 16 points per thread
     assert same_bits(gpu.model(), ref.model()), "initial model"
     for n in (120, 81):
         assert ref.iterate(n) == 0 and gpu.iterate(n) == 0
@@ -97,9 +97,9 @@ def test_raar_1024_then_er_bit_exact(lib, oracle_mod):
     assert gpu.iteration == ref.iteration == 221
     assert_same_state(gpu, ref)
     _check_efourier(gpu, ref, oracle_mod)
-    # the same run through the 16-point kernels
+    # the same run through the 8-point kernels
     other = setup_pattern(lib.Phaser((1024, 1024)), pat, RAAR, 0.87, sup)
-    other.set_tuning(SPLIT, 1)
+    other.set_tuning(SPLIT, 2)
     for n in (120, 81):
         assert other.iterate(n) == 0
     other.set_algorithm(ER, constraints=2)

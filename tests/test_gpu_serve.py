@@ -140,3 +140,89 @@ def test_job_larger_than_budget_fails_cleanly(lib):
             srv.result(big)
         with pytest.raises(RuntimeError):
             srv.submit(np.ones((8, 8), np.float32), np.ones((8, 8)), np.ones((8, 8)), [(9, 0.9, 10)])
+
+
+# ---- failure handling: a job that diverges, is cancelled or runs out of time
+# ends with its own status while the server and the other jobs carry on
+
+def test_nonfinite_job_fails_and_others_are_unaffected(lib):
+    """NaN amplitudes make every model non-finite after the first chunk: the
+    job ends as SPB_JOB_NONFINITE; the jobs beside it give their alone results
+    and the server takes new work afterwards."""
+    from libspimage_b200.serve import JOB_NONFINITE, Server
+
+    good = [JOBS[0], JOBS[1]]
+    with Server(max_active_jobs=3, chunk_slots=20) as srv:
+        amp, mask, support = _pattern((64, 64), 1)
+        bad_amp = amp.copy()
+        bad_amp[3, 5] = np.nan
+        bad = srv.submit(bad_amp, mask != 0, support, [(HIO, 0.9, 200)], starts=2, seed=3, support_period=20)
+        ids = [submit(srv, *j) for j in good]
+        info = srv.wait(bad, timeout=120)
+        assert info["status"] == JOB_NONFINITE
+        assert "NaN or infinite" in srv.job_error(bad)
+        with pytest.raises(RuntimeError, match="NaN or infinite"):
+            srv.result(bad)
+        results = []
+        for jid in ids:
+            assert srv.wait(jid, timeout=120)["status"] == 0, srv.job_error(jid)
+            results.append(srv.result(jid))
+        later = submit(srv, *JOBS[5])
+        assert srv.wait(later, timeout=120)["status"] == 0
+        later_res = srv.result(later)
+        st = srv.stats()
+    assert st["jobs_failed"] == 1
+    for res, job in zip(results, good):
+        _check(lib, res, *job)
+    _check(lib, later_res, *JOBS[5])
+
+
+def test_cancel_pending_and_running_jobs(lib):
+    from libspimage_b200.serve import JOB_CANCELLED, Server
+
+    with Server(max_active_jobs=1, chunk_slots=50) as srv:
+        long_id = submit(srv, (64, 64), [(HIO, 0.9, 400000)], 2, 7, 20, keep=False)
+        queued = submit(srv, (64, 64), [(HIO, 0.9, 40)], 2, 8, 20)
+        srv.cancel(queued)  # not admitted yet (one job at a time): ends at once
+        qinfo = srv.wait(queued, timeout=5)
+        assert qinfo["status"] == JOB_CANCELLED and qinfo["t_admit"] < 0
+        t0 = time.time()
+        while srv.wait(long_id, timeout=0.01)["t_admit"] < 0 and time.time() - t0 < 30:
+            pass
+        time.sleep(0.2)
+        srv.cancel(long_id)
+        info = srv.wait(long_id, timeout=60)
+        assert info["status"] == JOB_CANCELLED
+        assert info["t_finish"] - info["t_admit"] < 30
+        assert srv.job_error(long_id) == "cancelled"
+        with pytest.raises(RuntimeError, match="already ended"):
+            srv.cancel(long_id)
+        with pytest.raises(RuntimeError, match="unknown job"):
+            srv.cancel(123456)
+        # the cancelled job's context is reused by the next job of its shape
+        nxt = submit(srv, (64, 64), [(HIO, 0.9, 40)], 2, 9, 20)
+        assert srv.wait(nxt, timeout=60)["status"] == 0
+        res = srv.result(nxt)
+        st = srv.stats()
+    assert st["contexts_reused"] >= 1 and st["contexts_created"] == 1
+    _check(lib, res, (64, 64), [(HIO, 0.9, 40)], 2, 9, 20)
+
+
+def test_time_budget_expires_running_and_pending_jobs(lib):
+    from libspimage_b200.serve import JOB_EXPIRED, Server
+
+    amp, mask, support = _pattern((64, 64), 1)
+    with Server(max_active_jobs=1, chunk_slots=50) as srv:
+        first = srv.submit(amp, mask != 0, support, [(HIO, 0.9, 400000)], starts=2, seed=1, support_period=20,
+                           time_budget_s=0.5)
+        waiting = srv.submit(amp, mask != 0, support, [(HIO, 0.9, 40)], starts=2, seed=2, support_period=20,
+                             time_budget_s=0.001)
+        tiny = None
+        info = srv.wait(first, timeout=60)
+        assert info["status"] == JOB_EXPIRED and "time budget" in srv.job_error(first)
+        assert info["t_finish"] - info["t_submit"] < 30
+        winfo = srv.wait(waiting, timeout=60)
+        assert winfo["status"] == JOB_EXPIRED and winfo["t_admit"] < 0
+        tiny = srv.submit(amp, mask != 0, support, [(HIO, 0.9, 40)], starts=2, seed=3, support_period=20)
+        assert srv.wait(tiny, timeout=60)["status"] == 0
+        srv.result(tiny)
