@@ -12,4 +12,5 @@
 #include "spimage/image_filter.h"
 #include "spimage/support_update.h"
 #include "spimage/phasing.h"
+#include "spimage/prtf.h"
 #endif

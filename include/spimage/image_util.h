@@ -18,6 +18,11 @@ extern "C" {
 #define SP_COPY_MASK 2
 #define SP_COPY_ALL 3
 
+/* include/spimage/image_util.h:75-83 of the reference */
+typedef enum { SpFourierSpace = 1, SpRealSpace = 2 } SpSpace;
+typedef enum { SpInPlace = 65536, SpOutOfPlace = 131072 } SpPlace;
+typedef enum { SpEnantiomorph = 1, SpCorrectPhaseShift = 2 } SpSuperimposeFlags;
+
 Image *_sp_image_alloc(int x, int y, int z, const char *file, int line);
 #define sp_image_alloc(x, y, z) _sp_image_alloc(x, y, z, __FILE__, __LINE__)
 Image *_sp_image_duplicate(const Image *in, int flags, const char *file, int line);
@@ -31,6 +36,14 @@ void sp_image_dephase(Image *img);
 void sp_image_rephase(Image *img, int type);
 void sp_srand(int i);
 real p_drand48(void);
+/* Superimposes b on a with 1/precision-pixel precision (reference
+ * src/image_util.c:3024-3066): b is translated (Fourier translation) to the
+ * largest modulus of the cross-correlation of a and b computed on a grid
+ * padded precision times (2-D images are not padded along z); with
+ * SpEnantiomorph the reflected and conjugated b is taken when its
+ * correlation peak is higher; with SpCorrectPhaseShift b's constant phase is
+ * matched to a's at the peak.  On the GPU (spb_superimpose_fractional_host). */
+void sp_image_superimpose_fractional(Image *a, Image *b, SpSuperimposeFlags flags, int precision);
 
 static inline long long sp_image_size(const Image *a) {
   return (long long)a->image->x * a->image->y * a->image->z;

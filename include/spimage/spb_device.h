@@ -207,6 +207,22 @@ int spb_support_from_blur_host(long long n, const float *blur, int type, float v
  * with the reference to rounding, not bit for bit. */
 int spb_prtf_host(int nx, int ny, int nz, int n, const float *images, const int *supports, int flags, float *prtf,
                   float *super_image, int *super_mask);
+/* sp_image_superimpose_fractional (src/image_util.c:3024-3066) on host
+ * buffers: b ([N] complex) is overwritten with b superimposed on a.  flags:
+ * bit 0 SpEnantiomorph, bit 1 SpCorrectPhaseShift.  The correlation peaks,
+ * hence the translation and the enantiomorph choice, are the reference's
+ * (bit-identical FFTs and products); the Fourier translation and the phase
+ * shift evaluate cos/sin/atan2 in double on the GPU, so b agrees with the
+ * reference to rounding. */
+int spb_superimpose_fractional_host(int nx, int ny, int nz, const float *a, float *b, int flags, int precision);
+/* sp_prtf_basic (src/prtf.c:6-34) of n images ([n][N] complex) into out
+ * ([N] complex); bit for bit the reference's. */
+int spb_prtf_basic_host(int nx, int ny, int nz, int n, const float *images, float *out);
+/* sp_prtf_advanced (src/prtf.c:38-78) of n images ([n][N] complex, in
+ * Fourier space for space = 1, real space for 2) into prtf ([N] complex);
+ * write_back = 1 overwrites images with the superimposed images in their
+ * own space (SpInPlace). */
+int spb_prtf_advanced_host(int nx, int ny, int nz, int n, float *images, int space, int write_back, float *prtf);
 /* No counterpart in the reference.  spb_support_from_blur_host without any
  * device allocation, for callers that must not allocate device memory: a
  * process whose HBM is reserved up front by another allocator (a framework's

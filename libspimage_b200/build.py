@@ -22,7 +22,7 @@ BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libspimage_b200.so")
 
 CU_SOURCES = ["spb_kernels.cu", "spb_fast.cu", "spb_split.cu", "spb_capi.cu"]
-C_SOURCES = ["host/image.c", "host/phasing.c", "host/support_update.c", "host/fft.c"]
+C_SOURCES = ["host/image.c", "host/phasing.c", "host/support_update.c", "host/fft.c", "host/prtf.c"]
 CXX_SOURCES = ["host/serve.cpp"]
 HEADERS = ["spb_fft.cuh", "spb_internal.h", "spb_pointwise.cuh", "spb_passes.cuh"]
 

@@ -2145,3 +2145,261 @@ extern "C" int spb_prtf_host(int nx, int ny, int nz, int n, const float *images,
   spb_ctx_destroy(c);
   return rc;
 }
+
+// --------------------------------- fractional superposition and the C PRTFs
+// sp_image_superimpose_fractional (src/image_util.c:3024-3066), sp_prtf_basic
+// and sp_prtf_advanced (src/prtf.c:6-78) on the device.  The correlation
+// surfaces are the reference's bit for bit (same FFTs, same products and
+// scaling), so the argmax, the enantiomorph choice and the translation are the
+// reference's; the phase of the peak is taken on the host with the C library's
+// atan2 from the same float values.  The Fourier translation and the phase
+// shift evaluate cos, sin and atan2 in double on the GPU (the reference calls
+// the C library), so those steps agree to rounding, not always bit for bit.
+namespace spb {
+// zero_pad_shifted_image: source index along one axis of length n padded to p
+// (the spectrum split through its middle into the corners), -1 for a new zero
+__device__ __forceinline__ int pad_src(int x, int n, int p) {
+  if ((double)x < n / 2.0) return x;
+  if ((double)(p - x - 1) < (n - 1) / 2.0) return (n - 1) - (p - x - 1);
+  return -1;
+}
+__global__ void pad_shifted_kernel(const float2 *in, float2 *out, int nx, int ny, int nz, int px, int py, int pz) {
+  const long long n = (long long)px * py * pz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % px), y = (int)((i / px) % py), z = (int)(i / ((long long)px * py));
+    const int sx = pad_src(x, nx, px), sy = pad_src(y, ny, py), sz = pad_src(z, nz, pz);
+    out[i] = (sx < 0 || sy < 0 || sz < 0) ? make_float2(0.0f, 0.0f) : in[((long long)sz * ny + sy) * nx + sx];
+  }
+}
+__global__ void conj_kernel(float2 *v, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i].y = -v[i].y;
+}
+// sp_image_fourier_translate's multiplier (src/image_util.c:3249-3290): the
+// phase f_x*t_x*(1/nx)*2pi + f_y*t_y*(1/ny)*2pi + f_z*t_z*(1/nz)*2pi in float,
+// left to right, with f = k for k < n/2 else k - n (an axis of length 1 has
+// f = -1); (cos, -sin) in double rounded to float; sp_cmul's operation order
+__global__ void fourier_translate_kernel(float2 *F, int nx, int ny, int nz, float tx, float ty, float tz, float nxi,
+                                         float nyi, float nzi, float two_pi) {
+  const long long n = (long long)nx * ny * nz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
+    const int fx = x < nx / 2 ? x : -(nx - x), fy = y < ny / 2 ? y : -(ny - y), fz = z < nz / 2 ? z : -(nz - z);
+    const float ax = fmul(fmul(fmul((float)fx, tx), nxi), two_pi);
+    const float ay = fmul(fmul(fmul((float)fy, ty), nyi), two_pi);
+    const float az = fmul(fmul(fmul((float)fz, tz), nzi), two_pi);
+    const float arg = fadd(fadd(ax, ay), az);
+    const float c = (float)cos((double)arg), s = (float)(-sin((double)arg));
+    const float2 a = F[i];
+    F[i] = make_float2(fsub(fmul(a.x, c), fmul(a.y, s)), fadd(fmul(a.x, s), fmul(c, a.y)));
+  }
+}
+// sp_image_phase_shift in place (src/image_util.c:3413-3426)
+__global__ void phase_shift_kernel(float2 *v, long long n, float phi) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 a = v[i];
+    const float mag = cabs_ref(a);
+    const float arg = (float)atan2((double)a.y, (double)a.x);
+    const float t = fadd(arg, phi);
+    v[i] = make_float2((float)((double)mag * cos((double)t)), (float)((double)mag * sin((double)t)));
+  }
+}
+// sp_prtf_basic (src/prtf.c:6-34): per pixel the sum of the n images (added
+// in order to zeros) and the sum of their moduli; the sum scaled by 1/that
+// where it is not zero
+__global__ void prtf_basic_kernel(const float2 *imgs, long long N, int n, float2 *out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    float2 s = make_float2(0.0f, 0.0f);
+    float div = 0.0f;
+    for (int j = 0; j < n; j++) {
+      const float2 v = imgs[(long long)j * N + i];
+      s = make_float2(fadd(s.x, v.x), fadd(s.y, v.y));
+    }
+    for (int j = 0; j < n; j++) div = fadd(div, cabs_ref(imgs[(long long)j * N + i]));
+    if (div != 0.0f) {
+      const float sc = (float)__ddiv_rn(1.0, (double)div);  // 1.0/div in double, passed on as float
+      s = make_float2(fmul(s.x, sc), fmul(s.y, sc));
+    }
+    out[i] = s;
+  }
+}
+}  // namespace spb
+
+namespace {
+struct Superimposer {
+  spb_ctx *c = nullptr;   // the images' size
+  spb_ctx *cp = nullptr;  // the padded correlation size
+  float2 *PA = nullptr, *PB = nullptr, *PC = nullptr, *U = nullptr;
+  float *bval = nullptr;
+  long long *bidx = nullptr;
+  std::vector<float> hval;
+  std::vector<long long> hidx;
+  int precision = 1, pz = 1;
+  ~Superimposer() {
+    for (void *p : {(void *)PA, (void *)PB, (void *)PC, (void *)U, (void *)bval, (void *)bidx})
+      if (p) cudaFree(p);
+    spb_ctx_destroy(cp);
+    spb_ctx_destroy(c);
+  }
+  int init(int nx, int ny, int nz, int prec) {
+    if (prec < 1) return fail("superposition precision %d", prec);
+    precision = prec;
+    pz = nz > 1 ? prec : 1;  // 2-D images are not padded along z
+    if (spb_ctx_create(&c, nx, ny, nz) || spb_ctx_create(&cp, nx * prec, ny * prec, nz * pz)) return -1;
+    cp->st = c->st;  // one stream for both
+    const size_t np = sizeof(float2) * (size_t)cp->n;
+    CK(cudaMalloc(&PA, np));
+    CK(cudaMalloc(&PB, np));
+    CK(cudaMalloc(&PC, np));
+    CK(cudaMalloc(&U, sizeof(float2) * (size_t)c->n));
+    CK(cudaMalloc(&bval, sizeof(float) * 296));
+    CK(cudaMalloc(&bidx, sizeof(long long) * 296));
+    hval.resize(296);
+    hidx.resize(296);
+    return 0;
+  }
+  // sp_image_fft of an image, padded into the correlation grid
+  int padded_spectrum(const float2 *img, float2 *out) {
+    if (prtf_fft(c, img, U, -1)) return -1;
+    pad_shifted_kernel<<<1184, 256, 0, c->st>>>(U, out, c->nx, c->ny, c->nz, cp->nx, cp->ny, cp->nz);
+    CK(cudaGetLastError());
+    return 0;
+  }
+  // sp_image_convolute_fractional (src/image_util.c:1380-1461) of the padded
+  // spectra, then sp_image_max: largest modulus of the scaled surface, its
+  // first index and the scaled value there
+  int overlap(int conj, float *best, long long *best_i, float2 *val) {
+    prtf_cmul_kernel<<<1184, 256, 0, c->st>>>(PA, PB, PC, cp->n, conj);
+    CK(cudaGetLastError());
+    if (prtf_fft(cp, PC, PC, 1)) return -1;
+    const float s = (float)(1.0 / (double)c->n);  // the input's size scales, not the padded one
+    if (prtf_argmax(cp, PC, s, bval, bidx, hval.data(), hidx.data(), best, best_i)) return -1;
+    float2 raw;
+    CK(cudaMemcpy(&raw, PC + *best_i, sizeof(float2), cudaMemcpyDeviceToHost));
+    *val = make_float2(raw.x * s, raw.y * s);
+    return 0;
+  }
+  // superimposes b (device, the images' size) on a: src/image_util.c:3024-3066
+  int run(const float2 *a, float2 *b, int flags) {
+    if (padded_spectrum(a, PA) || padded_spectrum(b, PB)) return -1;
+    float m1, m2;
+    long long i1, i2;
+    float2 v1, v2;
+    if (overlap(1, &m1, &i1, &v1)) return -1;
+    const long long pxy = (long long)cp->nx * cp->ny;
+    int x = (int)(i1 % cp->nx), y = (int)((i1 % pxy) / cp->nx), z = (int)(i1 / pxy);
+    float phase = (float)atan2((double)v1.y, (double)v1.x);
+    bool flip = false;
+    if (flags & 1) {  // SpEnantiomorph
+      if (overlap(0, &m2, &i2, &v2)) return -1;
+      if (m2 > m1) {
+        x = (int)(i2 % cp->nx) + precision;
+        y = (int)((i2 % pxy) / cp->nx) + precision;
+        z = (int)(i2 / pxy) + precision;
+        phase = (float)atan2((double)v2.y, (double)v2.x);
+        flip = true;
+      }
+    }
+    if (flip) {  // the enantiomorph: reflected through the origin and conjugated
+      prtf_reflect_kernel<<<1184, 256, 0, c->st>>>(b, U, c->nx, c->ny, c->nz);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(b, U, sizeof(float2) * (size_t)c->n, cudaMemcpyDeviceToDevice, c->st));
+      conj_kernel<<<1184, 256, 0, c->st>>>(b, c->n);
+      CK(cudaGetLastError());
+    }
+    // sp_image_fourier_translate(b, x/p, y/p, z/p)
+    if (prtf_fft(c, b, U, -1)) return -1;
+    const float two_pi = (float)(2 * M_PI);
+    fourier_translate_kernel<<<1184, 256, 0, c->st>>>(
+        U, c->nx, c->ny, c->nz, (float)x / (float)precision, (float)y / (float)precision, (float)z / (float)precision,
+        (float)(1.0 / c->nx), (float)(1.0 / c->ny), (float)(1.0 / c->nz), two_pi);
+    CK(cudaGetLastError());
+    if (prtf_fft(c, U, b, 1)) return -1;
+    CK(launch_scale_cmul(b, c->n, (float)(1.0 / (double)c->n), c->st));  // sp_image_scale
+    if (flags & 2) {  // SpCorrectPhaseShift
+      phase_shift_kernel<<<1184, 256, 0, c->st>>>(b, c->n, phase);
+      CK(cudaGetLastError());
+    }
+    return 0;
+  }
+};
+}  // namespace
+
+extern "C" int spb_superimpose_fractional_host(int nx, int ny, int nz, const float *a, float *b, int flags,
+                                               int precision) {
+  Superimposer s;
+  if (s.init(nx, ny, nz, precision)) return -1;
+  const size_t nc = sizeof(float2) * (size_t)s.c->n;
+  float2 *da = nullptr, *db = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&da, nc) != cudaSuccess || cudaMalloc(&db, nc) != cudaSuccess) rc = fail("superimpose: cudaMalloc");
+  if (!rc && (cudaMemcpy(da, a, nc, cudaMemcpyHostToDevice) != cudaSuccess ||
+              cudaMemcpy(db, b, nc, cudaMemcpyHostToDevice) != cudaSuccess))
+    rc = fail("superimpose: upload");
+  if (!rc) rc = s.run(da, db, flags);
+  if (!rc && cudaMemcpy(b, db, nc, cudaMemcpyDeviceToHost) != cudaSuccess) rc = fail("superimpose: download");
+  if (da) cudaFree(da);
+  if (db) cudaFree(db);
+  return rc;
+}
+
+extern "C" int spb_prtf_basic_host(int nx, int ny, int nz, int n, const float *images, float *out) {
+  if (n < 1) return fail("prtf of %d images", n);
+  const long long N = (long long)nx * ny * nz;
+  if (N < 1) return fail("invalid image size");
+  float2 *d = nullptr, *o = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&d, sizeof(float2) * (size_t)(N * n)) != cudaSuccess || cudaMalloc(&o, sizeof(float2) * (size_t)N) != cudaSuccess)
+    rc = fail("prtf_basic: cudaMalloc");
+  if (!rc && cudaMemcpy(d, images, sizeof(float2) * (size_t)(N * n), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail("prtf_basic: upload");
+  if (!rc) {
+    prtf_basic_kernel<<<1184, 256>>>(d, N, n, o);
+    if (cudaGetLastError() != cudaSuccess) rc = fail("prtf_basic: launch");
+  }
+  if (!rc && cudaMemcpy(out, o, sizeof(float2) * (size_t)N, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail("prtf_basic: download");
+  if (d) cudaFree(d);
+  if (o) cudaFree(o);
+  return rc;
+}
+
+extern "C" int spb_prtf_advanced_host(int nx, int ny, int nz, int n, float *images, int space, int write_back,
+                                      float *prtf) {
+  if (n < 1) return fail("prtf of %d images", n);
+  if (space != 1 && space != 2) return fail("prtf_advanced: space must be 1 (Fourier) or 2 (real)");
+  Superimposer s;
+  if (s.init(nx, ny, nz, 4)) return -1;
+  spb_ctx *c = s.c;
+  const long long N = c->n;
+  const size_t all = sizeof(float2) * (size_t)(N * n);
+  float2 *R = nullptr, *F = nullptr, *o = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&R, all) != cudaSuccess || cudaMalloc(&F, all) != cudaSuccess ||
+      cudaMalloc(&o, sizeof(float2) * (size_t)N) != cudaSuccess)
+    rc = fail("prtf_advanced: cudaMalloc");
+  if (!rc && cudaMemcpyAsync(R, images, all, cudaMemcpyHostToDevice, c->st) != cudaSuccess) rc = fail("prtf_advanced: upload");
+  // images in Fourier space: their unnormalised inverse transforms (sp_image_ifft)
+  for (int i = 0; i < n && !rc && space == 1; i++) rc = prtf_fft(c, R + (size_t)i * N, R + (size_t)i * N, 1);
+  // every image superimposed on the first (SpCorrectPhaseShift | SpEnantiomorph, precision 4)
+  for (int i = 1; i < n && !rc; i++) rc = s.run(R, R + (size_t)i * N, 3);
+  // spectra scaled by 1/N (sp_image_fft, sp_image_scale), then sp_prtf_basic
+  for (int i = 0; i < n && !rc; i++) {
+    rc = prtf_fft(c, R + (size_t)i * N, F + (size_t)i * N, -1);
+    if (!rc && launch_scale_cmul(F + (size_t)i * N, N, (float)(1.0 / (double)N), c->st) != cudaSuccess)
+      rc = fail("prtf_advanced: scale");
+  }
+  if (!rc) {
+    prtf_basic_kernel<<<1184, 256, 0, c->st>>>(F, N, n, o);
+    if (cudaGetLastError() != cudaSuccess) rc = fail("prtf_advanced: launch");
+  }
+  if (!rc && cudaMemcpyAsync(prtf, o, sizeof(float2) * (size_t)N, cudaMemcpyDeviceToHost, c->st) != cudaSuccess)
+    rc = fail("prtf_advanced: download");
+  if (!rc && write_back &&
+      cudaMemcpyAsync(images, space == 1 ? F : R, all, cudaMemcpyDeviceToHost, c->st) != cudaSuccess)
+    rc = fail("prtf_advanced: download");
+  if (cudaStreamSynchronize(c->st) != cudaSuccess && !rc) rc = fail("prtf_advanced: device error");
+  for (void *p : {(void *)R, (void *)F, (void *)o})
+    if (p) cudaFree(p);
+  return rc;
+}

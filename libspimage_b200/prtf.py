@@ -68,3 +68,64 @@ def prtf(images_rs, supports, translate=True, enantio=True, full_out=False):
         out["prtf_r"] = radial_mean(out["prtf"])
         out["super_mask"] = out_msk > 0
     return out
+
+
+# ---- the reference's C PRTF and fractional superposition (include/spimage/prtf.h,
+# sp_image_superimpose_fractional), on the GPU
+
+def _bind_c(lib):
+    if not getattr(lib, "_cprtf_bound", False):
+        fp = C.POINTER(C.c_float)
+        lib.spb_superimpose_fractional_host.restype = C.c_int
+        lib.spb_superimpose_fractional_host.argtypes = [C.c_int, C.c_int, C.c_int, fp, fp, C.c_int, C.c_int]
+        lib.spb_prtf_basic_host.restype = C.c_int
+        lib.spb_prtf_basic_host.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, fp, fp]
+        lib.spb_prtf_advanced_host.restype = C.c_int
+        lib.spb_prtf_advanced_host.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_int, fp]
+        lib._cprtf_bound = True
+    return lib
+
+
+def _dims(shape):
+    nz, ny, nx = (1,) + tuple(shape) if len(shape) == 2 else tuple(shape)
+    return nx, ny, nz
+
+
+def superimpose_fractional(a, b, flags=3, precision=4):
+    """b superimposed on a (sp_image_superimpose_fractional): flags bit 0
+    SpEnantiomorph, bit 1 SpCorrectPhaseShift."""
+    lib = _bind_c(load())
+    fp = C.POINTER(C.c_float)
+    a = np.ascontiguousarray(a, np.complex64)
+    out = np.ascontiguousarray(b, np.complex64).copy()
+    rc = lib.spb_superimpose_fractional_host(*_dims(a.shape), a.ctypes.data_as(fp), out.ctypes.data_as(fp), int(flags),
+                                             int(precision))
+    if rc != 0:
+        raise RuntimeError(lib.spb_error_string().decode())
+    return out
+
+
+def prtf_basic(images):
+    """sp_prtf_basic of images[n, ...] (complex, Fourier space)."""
+    lib = _bind_c(load())
+    fp = C.POINTER(C.c_float)
+    ims = np.ascontiguousarray(images, np.complex64)
+    out = np.zeros(ims.shape[1:], np.complex64)
+    rc = lib.spb_prtf_basic_host(*_dims(ims.shape[1:]), ims.shape[0], ims.ctypes.data_as(fp), out.ctypes.data_as(fp))
+    if rc != 0:
+        raise RuntimeError(lib.spb_error_string().decode())
+    return out
+
+
+def prtf_advanced(images, fourier_space=True, in_place=False):
+    """(prtf, images) of sp_prtf_advanced; images are overwritten with the
+    superimposed images when in_place."""
+    lib = _bind_c(load())
+    fp = C.POINTER(C.c_float)
+    ims = np.ascontiguousarray(images, np.complex64).copy()
+    out = np.zeros(ims.shape[1:], np.complex64)
+    rc = lib.spb_prtf_advanced_host(*_dims(ims.shape[1:]), ims.shape[0], ims.ctypes.data_as(fp),
+                                    1 if fourier_space else 2, 1 if in_place else 0, out.ctypes.data_as(fp))
+    if rc != 0:
+        raise RuntimeError(lib.spb_error_string().decode())
+    return out, ims

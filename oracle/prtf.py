@@ -106,3 +106,58 @@ def prtf_reference(images_rs, supports, translate=True, enantio=True):
            "super_mask": avg_msk > 0}
     avg.free()
     return out
+
+
+# ---- the reference's C PRTF (src/prtf.c:6-78) and fractional superposition
+# (src/image_util.c:3024-3066), called in oracle/_ref
+
+def _c_lib():
+    lib = _lib()
+    if not getattr(lib, "_cprtf_bound", False):
+        lib.sp_prtf_basic.argtypes = [C.POINTER(_vp), C.c_int]
+        lib.sp_prtf_basic.restype = _vp
+        lib.sp_prtf_advanced.argtypes = [C.POINTER(_vp), C.c_int, C.c_int]
+        lib.sp_prtf_advanced.restype = _vp
+        lib.sp_image_superimpose_fractional.argtypes = [_vp, _vp, C.c_int, C.c_int]
+        lib._cprtf_bound = True
+    return lib
+
+
+def superimpose_fractional(a, b, flags, precision):
+    """b superimposed on a (both numpy, same shape) by the reference."""
+    lib = _c_lib()
+    ia, ib = _Img(lib, np.asarray(a)), _Img(lib, np.asarray(b))
+    lib.sp_image_superimpose_fractional(ia.h, ib.h, int(flags), int(precision))
+    out = ib.data()
+    ia.free()
+    ib.free()
+    return out
+
+
+def prtf_basic(images):
+    lib = _c_lib()
+    imgs = [_Img(lib, np.asarray(im)) for im in images]
+    arr = (_vp * len(imgs))(*[im.h for im in imgs])
+    h = lib.sp_prtf_basic(arr, len(imgs))
+    out = _Img.data_of(lib, h, imgs[0].n, imgs[0].shape)
+    lib.ref_image_free(h)
+    for im in imgs:
+        im.free()
+    return out
+
+
+def prtf_advanced(images, flags):
+    """(prtf, images after the call) of the reference's sp_prtf_advanced; the
+    inputs are marked phased and shifted (as spectra from sp_image_fft are)."""
+    lib = _c_lib()
+    imgs = [_Img(lib, np.asarray(im)) for im in images]
+    for im in imgs:
+        lib.ref_image_set_flags(im.h, 1, 1)
+    arr = (_vp * len(imgs))(*[im.h for im in imgs])
+    h = lib.sp_prtf_advanced(arr, len(imgs), int(flags))
+    out = _Img.data_of(lib, h, imgs[0].n, imgs[0].shape)
+    lib.ref_image_free(h)
+    after = [im.data() for im in imgs]
+    for im in imgs:
+        im.free()
+    return out, after
