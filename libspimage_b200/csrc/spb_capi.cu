@@ -2274,8 +2274,9 @@ struct Superimposer {
     if (prtf_fft(cp, PC, PC, 1)) return -1;
     const float s = (float)(1.0 / (double)c->n);  // the input's size scales, not the padded one
     if (prtf_argmax(cp, PC, s, bval, bidx, hval.data(), hidx.data(), best, best_i)) return -1;
-    float2 raw;
-    CK(cudaMemcpy(&raw, PC + *best_i, sizeof(float2), cudaMemcpyDeviceToHost));
+    float2 raw;  // (prtf_argmax has synchronised the stream)
+    CK(cudaMemcpyAsync(&raw, PC + *best_i, sizeof(float2), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
     *val = make_float2(raw.x * s, raw.y * s);
     return 0;
   }
@@ -2333,11 +2334,14 @@ extern "C" int spb_superimpose_fractional_host(int nx, int ny, int nz, const flo
   float2 *da = nullptr, *db = nullptr;
   int rc = 0;
   if (cudaMalloc(&da, nc) != cudaSuccess || cudaMalloc(&db, nc) != cudaSuccess) rc = fail("superimpose: cudaMalloc");
-  if (!rc && (cudaMemcpy(da, a, nc, cudaMemcpyHostToDevice) != cudaSuccess ||
-              cudaMemcpy(db, b, nc, cudaMemcpyHostToDevice) != cudaSuccess))
+  // everything on the context's stream (non-blocking: the legacy stream
+  // would not wait for it)
+  if (!rc && (cudaMemcpyAsync(da, a, nc, cudaMemcpyHostToDevice, s.c->st) != cudaSuccess ||
+              cudaMemcpyAsync(db, b, nc, cudaMemcpyHostToDevice, s.c->st) != cudaSuccess))
     rc = fail("superimpose: upload");
   if (!rc) rc = s.run(da, db, flags);
-  if (!rc && cudaMemcpy(b, db, nc, cudaMemcpyDeviceToHost) != cudaSuccess) rc = fail("superimpose: download");
+  if (!rc && cudaMemcpyAsync(b, db, nc, cudaMemcpyDeviceToHost, s.c->st) != cudaSuccess) rc = fail("superimpose: download");
+  if (cudaStreamSynchronize(s.c->st) != cudaSuccess && !rc) rc = fail("superimpose: device error");
   if (da) cudaFree(da);
   if (db) cudaFree(db);
   return rc;
