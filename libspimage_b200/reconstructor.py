@@ -116,14 +116,14 @@ class Reconstructor:
         self._free()
         self._amplitudes = None
         self._mask = None
-        self._initial_support_config = None
-        self._number_of_iterations = None
-        self._number_of_outputs_images = None
-        self._number_of_outputs_scores = None
-        self._support_algorithms_configs = []
-        self._i_support_algorithms = None
-        self._phasing_algorithms_configs = []
-        self._i_phasing_algorithms = None
+        self._support_init_args = None
+        self._n_iterations = None
+        self._n_image_outputs = None
+        self._n_score_outputs = None
+        self._support_stages = []
+        self._support_stage_idx = None
+        self._phasing_stages = []
+        self._phasing_stage_idx = None
         self._reconstruction = None
         self._iteration = None
 
@@ -149,7 +149,7 @@ class Reconstructor:
         (zero frequency at the centre) unless shifted=True."""
         A = np.array(intensities, dtype="float")
         if (A < 0).sum() > 0:
-            self._log("Intensities found that have negative values. These values are set to zero.")
+            self._log("negative intensities clipped to zero")
             A[A < 0] = 0.
         A = np.sqrt(A)
         self._amplitudes = A if shifted else np.fft.fftshift(A)
@@ -160,30 +160,29 @@ class Reconstructor:
         self._mask = M if shifted else np.fft.fftshift(M)
 
     def set_number_of_iterations(self, number_of_iterations):
-        self._number_of_iterations = number_of_iterations
+        self._n_iterations = number_of_iterations
 
     def set_number_of_outputs_images(self, number_of_outputs_images):
-        self._number_of_outputs_images = number_of_outputs_images
+        self._n_image_outputs = number_of_outputs_images
 
     def set_number_of_outputs_scores(self, number_of_outputs_scores):
-        self._number_of_outputs_scores = number_of_outputs_scores
+        self._n_score_outputs = number_of_outputs_scores
 
     def set_number_of_outputs(self, number_of_outputs):
-        self._number_of_outputs_images = number_of_outputs
-        self._number_of_outputs_scores = number_of_outputs
+        self._n_image_outputs = number_of_outputs
+        self._n_score_outputs = number_of_outputs
 
     def set_initial_support(self, **kwargs):
         """radius=..., area=... (fraction of the image) or support_mask=... (used as given)."""
         for k in ("radius", "area", "support_mask"):
             if k in kwargs:
-                self._initial_support_config = {k: kwargs[k]}
+                self._support_init_args = {k: kwargs[k]}
                 return
-        self._log("set_initial_support requires one of the following key word arguments: radius, area, "
-                  "support_mask", "ERROR")
+        self._log("set_initial_support: give one of radius, area or support_mask", "ERROR")
 
     def set_support_algorithm(self, type, number_of_iterations=None, center_image=False, **kwargs):
-        self._support_algorithms_configs = []
-        self._i_support_algorithms = None
+        self._support_stages = []
+        self._support_stage_idx = None
         self.append_support_algorithm(type, number_of_iterations=number_of_iterations, center_image=center_image,
                                       **kwargs)
 
@@ -191,26 +190,26 @@ class Reconstructor:
         """area: update_period, blur_init, blur_final, area_init, area_final;
         threshold: update_period, blur_init, blur_final, threshold_init, threshold_final; static."""
         conf = {"type": type, "center_image": center_image, "number_of_iterations": number_of_iterations}
-        if number_of_iterations is None and len(self._support_algorithms_configs) > 0:
-            self._log("You can not have more than one support algorithm of unspecified number of iterations.", "ERROR")
+        if number_of_iterations is None and len(self._support_stages) > 0:
+            self._log("only one support stage may leave its number of iterations open", "ERROR")
             return
         if type not in _SUPPORT_KWARGS:
-            self._log("append_support_algorithm accepts: " + str(list(_SUPPORT_KWARGS)), "ERROR")
+            self._log("append_support_algorithm: known arguments are " + str(list(_SUPPORT_KWARGS)), "ERROR")
             return
         for k in _SUPPORT_KWARGS[type]:
             if k not in kwargs:
-                self._log("append_support_algorithm (%s) requires the argument %s" % (type, k), "ERROR")
+                self._log("append_support_algorithm: %s needs %s" % (type, k), "ERROR")
                 return
             conf[k] = kwargs[k]
         if number_of_iterations is not None:
-            if not self._support_algorithms_configs:
-                self._i_support_algorithms = 0
-            self._i_support_algorithms += number_of_iterations
-        self._support_algorithms_configs.append(conf)
+            if not self._support_stages:
+                self._support_stage_idx = 0
+            self._support_stage_idx += number_of_iterations
+        self._support_stages.append(conf)
 
     def set_phasing_algorithm(self, type, **kwargs):
-        self._phasing_algorithms_configs = []
-        self._i_phasing_algorithms = None
+        self._phasing_stages = []
+        self._phasing_stage_idx = None
         kw = dict(kwargs)
         kw.setdefault("number_of_iterations", None)
         self.append_phasing_algorithm(type, **kw)
@@ -220,26 +219,26 @@ class Reconstructor:
         gamma1, gamma2; all take number_of_iterations and constraints (a list of
         enforce_positivity, enforce_real, enforce_centrosymmetry)."""
         if "number_of_iterations" not in kwargs:
-            self._log("append_phasing_algorithm requires the keyword argument 'number_of_iterations'.", "ERROR")
+            self._log("append_phasing_algorithm: number_of_iterations is required", "ERROR")
             return
         n = kwargs["number_of_iterations"]
-        if n is None and len(self._phasing_algorithms_configs) > 0:
-            self._log("You can not have more than one phasing algorithm of unspecified number of iterations.", "ERROR")
+        if n is None and len(self._phasing_stages) > 0:
+            self._log("only one phasing stage may leave its number of iterations open", "ERROR")
             return
         if type not in _PHASING_KWARGS:
-            self._log("append_phasing_algorithm accepts: %s" % list(_PHASING_KWARGS), "ERROR")
+            self._log("append_phasing_algorithm: known arguments are %s" % list(_PHASING_KWARGS), "ERROR")
             return
         for k in _PHASING_KWARGS[type]:
             if k not in kwargs:
-                self._log("append_phasing_algorithm (%s) requires the argument %s" % (type, k), "ERROR")
+                self._log("append_phasing_algorithm: %s needs %s" % (type, k), "ERROR")
                 return
         conf = {"type": type, "constraints": kwargs.get("constraints", "")}
         conf.update(kwargs)
         if n is not None:
-            if not self._phasing_algorithms_configs:
-                self._i_phasing_algorithms = 0
-            self._i_phasing_algorithms += n
-        self._phasing_algorithms_configs.append(conf)
+            if not self._phasing_stages:
+                self._phasing_stage_idx = 0
+            self._phasing_stage_idx += n
+        self._phasing_stages.append(conf)
 
     # ------------------------------------------------------------- preparation
     def _prepare(self):
@@ -248,25 +247,25 @@ class Reconstructor:
         when the configuration is incomplete."""
         ok = True
         if self._amplitudes is None:
-            self._log("Reconstruction cannot start! You need to set the intensities.", "ERROR")
+            self._log("not ready: no intensities set", "ERROR")
             ok = False
-        if self._initial_support_config is None:
-            self._log("Reconstruction cannot start! You need to set the initial support.", "ERROR")
+        if self._support_init_args is None:
+            self._log("not ready: no initial support set", "ERROR")
             ok = False
-        if not self._support_algorithms_configs:
-            self._log("Reconstruction cannot start! You need to set the support algorithm.", "ERROR")
+        if not self._support_stages:
+            self._log("not ready: no support algorithm set", "ERROR")
             ok = False
-        if not self._phasing_algorithms_configs:
-            self._log("Reconstruction cannot start! You need to set the phasing algorithm.", "ERROR")
+        if not self._phasing_stages:
+            self._log("not ready: no phasing algorithm set", "ERROR")
             ok = False
-        if self._number_of_outputs_images is None or self._number_of_outputs_scores is None:
-            self._log("Cannot prepare reconstruction. Number of outputs need to be set.", "ERROR")
+        if self._n_image_outputs is None or self._n_score_outputs is None:
+            self._log("not ready: number of outputs not set", "ERROR")
             ok = False
-        if self._i_support_algorithms is not None and self._i_support_algorithms != self._number_of_iterations:
-            self._log("Support algorithms are not in line with the set number of iterations.", "ERROR")
+        if self._support_stage_idx is not None and self._support_stage_idx != self._n_iterations:
+            self._log("the support stages do not add up to the number of iterations", "ERROR")
             ok = False
-        if self._i_phasing_algorithms is not None and self._i_phasing_algorithms != self._number_of_iterations:
-            self._log("Phasing algorithms are not in line with the set number of iterations.", "ERROR")
+        if self._phasing_stage_idx is not None and self._phasing_stage_idx != self._n_iterations:
+            self._log("the phasing stages do not add up to the number of iterations", "ERROR")
             ok = False
         if ok and not self._use_gpu:
             raise RuntimeError("use_gpu=False: this library runs phasing on the GPU only")
@@ -277,9 +276,9 @@ class Reconstructor:
         (src/_spimage_reconstructor.py:452-533): beta, blur and area schedules
         run from the algorithm's first to its last iteration."""
         lib = self._lib
-        N = self._number_of_iterations
+        N = self._n_iterations
         sups, i = [], 0
-        for conf in self._support_algorithms_configs:
+        for conf in self._support_stages:
             n = conf["number_of_iterations"] if conf["number_of_iterations"] is not None else N
             period = conf.get("update_period")
             if conf["type"] == "area":
@@ -297,7 +296,7 @@ class Reconstructor:
             sups.append((arr, n))
             i += n
         algs, i = [], 0
-        for conf in self._phasing_algorithms_configs:
+        for conf in self._phasing_stages:
             n = conf["number_of_iterations"] if conf["number_of_iterations"] is not None else N
             c = phasing_constraints(conf.get("constraints", ""))
             if conf["type"] in ("raar", "hio", "diffmap"):
@@ -328,7 +327,7 @@ class Reconstructor:
         A = self._amplitudes
         M = self._mask if self._mask is not None else np.ones(A.shape, bool)
         amp = self._image(A, M.astype(np.int32))
-        support = initial_support_mask(A.shape, **self._initial_support_config)
+        support = initial_support_mask(A.shape, **self._support_init_args)
         self._initial_support = support
         sup_img = self._image(support)
         ph = lib.sp_phaser_alloc()
@@ -423,9 +422,9 @@ class Reconstructor:
         for `starts` starts at once; returns one output dictionary per start."""
         algs, sups = self._start(starts)
         lib, ph = self._lib, self._ph
-        N = self._number_of_iterations
-        out_img = output_iterations(N, self._number_of_outputs_images)
-        out_sco = output_iterations(N, self._number_of_outputs_scores)
+        N = self._n_iterations
+        out_img = output_iterations(N, self._n_image_outputs)
+        out_sco = output_iterations(N, self._n_score_outputs)
         shape = self._amplitudes.shape
         res = [{"real_space": np.zeros((len(out_img),) + shape, np.complex128),
                 "support": np.zeros((len(out_img),) + shape, bool),
