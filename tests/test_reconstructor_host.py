@@ -44,11 +44,11 @@ def test_incomplete_configuration_returns_none():
     R.set_support_algorithm("area", update_period=5, blur_init=2., blur_final=1., area_init=.1, area_final=.1)
     assert R.reconstruct() is None                     # no phasing algorithm
     R.set_phasing_algorithm("hio", beta_init=0.9)      # beta_final missing: rejected
-    assert R._phasing_algorithms_configs == []
+    assert R._phasing_stages == []
     R.append_phasing_algorithm("hio", number_of_iterations=6, beta_init=.9, beta_final=.9)
     assert R.reconstruct() is None                     # 6 of 10 iterations covered
     R.append_support_algorithm("threshold", number_of_iterations=5, update_period=5, blur_init=2.)
-    assert len(R._support_algorithms_configs) == 1     # missing arguments: rejected
+    assert len(R._support_stages) == 1     # missing arguments: rejected
 
 
 def test_negative_intensities_and_shift():
