@@ -85,9 +85,20 @@ const char *spb_kernel_name(int kind);
  * the iteration's two passes holds: 1 = 16 (the 16-point kernels), 2 = 8 (the
  * 8-point kernels, twice the threads per line, for lengths 256, 512, 1024 and
  * 4096), 0 the built-in choice (8 when the 16-point kernels would give the
- * SMs fewer than 8 warps of lines).  Setting a knob drops the context's
- * captured graphs. */
-enum { SPB_TUNE_ROW_LINES = 0, SPB_TUNE_NO_PDL = 1, SPB_TUNE_ROW_G0 = 2, SPB_TUNE_SPLIT = 3, SPB_TUNE_KNOBS = 4 };
+ * SMs fewer than 8 warps of lines); SPB_TUNE_PERSIST = 2 runs the
+ * iterations of a call of a 32x32, 64x64 or 128x128 pattern (HIO, RAAR or
+ * ER; modulus projection without error margins) in one launch, one block per
+ * start holding its spectrum in shared memory, 1 = the two-pass kernels,
+ * 0 the built-in choice.  Setting a knob drops the context's captured
+ * graphs. */
+enum {
+  SPB_TUNE_ROW_LINES = 0,
+  SPB_TUNE_NO_PDL = 1,
+  SPB_TUNE_ROW_G0 = 2,
+  SPB_TUNE_SPLIT = 3,
+  SPB_TUNE_PERSIST = 4,
+  SPB_TUNE_KNOBS = 5
+};
 int spb_ctx_set_tuning(spb_ctx *ctx, int knob, int value);
 int spb_ctx_get_tuning(spb_ctx *ctx, int knob);
 /* Autotuner (no reference counterpart): times `calls` calls of `iterations`

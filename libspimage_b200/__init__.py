@@ -500,7 +500,8 @@ class Phaser:
         _check(self.lib.sp_phaser_autotune(self.ph), "sp_phaser_autotune")
         ctx = self.lib.sp_phaser_device_context(self.ph)
         return {"row_lines": self.lib.spb_ctx_get_tuning(ctx, 0), "no_pdl": self.lib.spb_ctx_get_tuning(ctx, 1),
-                "row_g0": self.lib.spb_ctx_get_tuning(ctx, 2), "split": self.lib.spb_ctx_get_tuning(ctx, 3)}
+                "row_g0": self.lib.spb_ctx_get_tuning(ctx, 2), "split": self.lib.spb_ctx_get_tuning(ctx, 3),
+                "persist": self.lib.spb_ctx_get_tuning(ctx, 4)}
 
     def set_tuning(self, knob, value):
         ctx = self.lib.sp_phaser_device_context(self.ph)

@@ -941,6 +941,20 @@ extern "C" int spb_ctx_mask_out_unmeasured(spb_ctx *c) {
   return 0;
 }
 
+// whether the persistent form applies to this context and algorithm
+static bool persist_wanted_shape(const spb_ctx *c, const spb_alg_desc *alg) {
+  if (c->nz != 1 || c->nx != c->ny || (c->nx != 32 && c->nx != 64 && c->nx != 128)) return false;
+  if (alg->algorithm == ALG_DM || alg->objective != 0 || (alg->constraints & C_MARGIN)) return false;
+  return c->amp_line && c->meas_bits;
+}
+
+// The built-in choice between the persistent and the two-pass forms of a
+// supported pattern (measured on one B200; see persist_wanted).
+static bool persist_auto(const spb_ctx *c) {
+  (void)c;
+  return false;
+}
+
 // One iteration of every start: g0 <- g1 (buffer roles swap), X -> Y
 // (projection pass) -> row pass writing g1 and the next X.  `a` carries the
 // algorithm scalars.
@@ -1076,6 +1090,16 @@ static int upload_betas(spb_ctx *c, const float *beta, int n) {
   return 0;
 }
 
+// The persistent form for this call: asked for (knob 2) or the built-in
+// choice, on a 32x32, 64x64 or 128x128 pattern with HIO, RAAR or ER and the
+// plain modulus projection (line-major operands built); never while per-kernel
+// profiling is on.
+static bool persist_wanted(const spb_ctx *c, const spb_alg_desc *alg) {
+  const int k = c->tune[SPB_TUNE_PERSIST];
+  if (k == 1 || c->prof.on || !persist_wanted_shape(c, alg)) return false;
+  return k == 2 ? true : persist_auto(c);
+}
+
 extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float *beta, int iterations,
                                int keep_gp) {
   if (iterations <= 0) return 0;
@@ -1108,6 +1132,21 @@ extern "C" int spb_ctx_iterate(spb_ctx *c, const spb_alg_desc *alg, const float 
   a.one_p_g2 = 1 + alg->gamma2;
   a.size_f = (float)(int)c->n;
   a.inv_size_pow2 = (c->n & (c->n - 1)) == 0 ? (float)(1.0 / (double)c->n) : 0.0f;
+  // small square patterns: every iteration of the call in one launch, one
+  // block per start with its spectrum resident
+  if (persist_wanted(c, alg)) {
+    if (upload_betas(c, beta, iterations)) return -1;
+    PassArgs p = a;
+    p.beta_tab = c->beta_dev;
+    p.beta_base = c->beta_zero;
+    p.dst = c->X;
+    p.gp = c->gp;
+    CK(launch_persist(c->ax.lp, p, c->g[0], c->g[1], c->cur, iterations, keep_gp, c->nb, c->st));
+    c->launches++;
+    c->cur ^= (iterations & 1);
+    c->xf_valid = 0;
+    return 0;
+  }
   // a short call (one support period, typically) runs as one captured graph
   if (c->use_graphs && !c->prof.on && c->warm_alg[A] && iterations >= 2 && iterations <= kWholeGraphMax) {
     GraphEntry *g = find_graph(c, alg, iterations, keep_gp);
@@ -1415,13 +1454,14 @@ struct TuneKey {
 };
 std::mutex g_tune_mu;
 struct TuneChoice {
-  int lines, nopdl, g0, split;
+  int lines, nopdl, g0, split, persist;
 };
 std::map<TuneKey, TuneChoice> g_tune_cache;
 
 int apply_choice(spb_ctx *c, const TuneChoice &t) {
   if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, t.lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, t.nopdl) ||
-      spb_ctx_set_tuning(c, SPB_TUNE_ROW_G0, t.g0) || spb_ctx_set_tuning(c, SPB_TUNE_SPLIT, t.split))
+      spb_ctx_set_tuning(c, SPB_TUNE_ROW_G0, t.g0) || spb_ctx_set_tuning(c, SPB_TUNE_SPLIT, t.split) ||
+      spb_ctx_set_tuning(c, SPB_TUNE_PERSIST, t.persist))
     return -1;
   return 0;
 }
@@ -1453,7 +1493,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   const int cur0 = c->cur, xv0 = c->x_valid, xfv0 = c->xf_valid;
   const float xfg0 = c->xf_gamma1;
   const TuneChoice knob0{c->tune[SPB_TUNE_ROW_LINES], c->tune[SPB_TUNE_NO_PDL], c->tune[SPB_TUNE_ROW_G0],
-                         c->tune[SPB_TUNE_SPLIT]};
+                         c->tune[SPB_TUNE_SPLIT], c->tune[SPB_TUNE_PERSIST]};
   int rc = 0;
   const float2 *bufs[4] = {c->g[0], c->g[1], c->gp, c->X};
   for (int k = 0; k < 4 && !rc; k++)
@@ -1468,18 +1508,25 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   const int T = c->nx >= 16 ? c->nx / 16 : 1;
   const int lpb_max = 256 / T > 0 ? 256 / T : 1;
   double best = 1e30;
-  TuneChoice bestc{0, 0, 0, 0};
+  TuneChoice bestc{0, 0, 0, 0, 1};
   // 8-point kernels exist for these row (x) and projection-axis lengths
   auto split_len = [](int n) { return n == 256 || n == 512 || n == 1024 || n == 4096; };
   const bool can_split = split_len(c->nx) || split_len(c->nz > 1 ? c->nz : c->ny);
-  for (int cand = 0; cand < 2 * 2 * 2 * 16 && !rc; cand++) {
-    const int nopdl = cand & 1, g0 = 1 + ((cand >> 1) & 1), sp = 1 + ((cand >> 2) & 1), li = cand >> 3;
+  const bool can_persist = persist_wanted_shape(c, alg);
+  // the two-pass launch shapes, then (where it applies) the persistent form,
+  // which has no launch-shape knobs of its own
+  for (int cand = 0; cand < 2 * 2 * 2 * 16 + 1 && !rc; cand++) {
+    const bool pcand = cand == 2 * 2 * 2 * 16;
+    if (pcand && !can_persist) continue;
+    const int nopdl = pcand ? 0 : cand & 1, g0 = pcand ? 1 : 1 + ((cand >> 1) & 1);
+    const int sp = pcand ? 1 : 1 + ((cand >> 2) & 1), li = pcand ? 0 : cand >> 3;
     const int lines = li ? 1 << (li - 1) : 0;
     if (lines > lpb_max) continue;  // (0 is the built-in choice, which may be lpb_max or fewer)
     // the 8-point row kernel has one block shape: no lines-per-block candidates
     if (sp == 2 && (!can_split || li != 0)) continue;
+    const int pe = pcand ? 2 : 1;
     {
-      if (apply_choice(c, TuneChoice{lines, nopdl, g0, sp})) {
+      if (apply_choice(c, TuneChoice{lines, nopdl, g0, sp, pe})) {
         rc = -1;
         break;
       }
@@ -1494,7 +1541,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
         rc = fail("autotune: timing failed");
       if (!rc && ms < best) {
         best = ms;
-        bestc = TuneChoice{lines, nopdl, g0, sp};
+        bestc = TuneChoice{lines, nopdl, g0, sp, pe};
       }
     }
   }

@@ -477,6 +477,169 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
     for (int q = 0; q < 16; q++) a.dst[lbase + q * qstride] = v[q];
 }
 
+// ------------------------------------------------ persistent small patterns
+// One block per start of an N x N pattern (N = 32, 64, 128) runs every
+// iteration of a call with the start's spectrum resident in shared memory:
+// X (the row transform of the model) stays in the block between iterations,
+// and each iteration is the column pass (forward y, projection, inverse y)
+// and the row pass (inverse x, update, forward x) of the two-pass kernels,
+// separated by block barriers instead of kernel boundaries.  The previous
+// iterate, the flags and the amplitude lines are read from global memory
+// (L2); the new iterate is written there.  Same transforms and pointwise
+// steps, so the bits are those of the two-pass kernels.
+//
+// Shared memory: [twiddles N][N rows of pitch P = N + N/16].  Element (row i,
+// column x) of X sits at i*P + x; a row's exchanges use the padded positions
+// of its own P slots, a column's exchanges use its own elements (stride P).
+namespace reg {
+template <int N, int S, int NS, bool INV, int STRIDE>
+struct PStages {
+  // storage address of line index i: padded within a row (STRIDE 0) or down a column
+  static __device__ __forceinline__ int at(int i) { return STRIDE == 0 ? pad(i) : i * STRIDE; }
+  static __device__ __forceinline__ void run(float2 (&v)[16], float2 *line, int t, const float2 *stw) {
+    constexpr int R = plan_radix(N, S);
+    constexpr int T = N / 16;
+    constexpr int J = 16 / R;
+    constexpr bool LAST = (S == plan_len(N) - 1);
+#pragma unroll
+    for (int j = 0; j < J; j++) {
+      float2 a[R];
+#pragma unroll
+      for (int m = 0; m < R; m++) a[m] = v[j + m * J];
+      const int b = t + T * j;
+      const int k = b & (NS - 1);
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int m = 1; m < R; m++) {
+          float2 w = stw[(m - 1) * NS + k];
+          if (INV) w.y = -w.y;
+          const float2 p = cmulw(a[m], w.x, w.y);
+          a[m] = k ? p : a[m];
+        }
+      }
+      bfly<R, INV>(a);
+      if constexpr (LAST) {
+#pragma unroll
+        for (int m = 0; m < R; m++) v[j + m * J] = a[m];
+      } else {
+        const int base = (b / NS) * NS * R + k;
+#pragma unroll
+        for (int m = 0; m < R; m++) line[at(base + m * NS)] = a[m];
+      }
+    }
+    if constexpr (!LAST) {
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] = line[at(t + T * q)];
+      __syncthreads();
+      PStages<N, S + 1, NS * R, INV, STRIDE>::run(v, line, t, stw + (R - 1) * NS);
+    }
+  }
+};
+}  // namespace reg
+
+// blocks per SM the register budget is sized for (64 registers a thread)
+template <int N>
+__host__ __device__ constexpr int persist_min_blocks() {
+  return N >= 128 ? 1 : (N == 64 ? 4 : 16);
+}
+
+template <int N>
+__global__ void __launch_bounds__(N * N / 16, persist_min_blocks<N>())
+    persist_kernel(PassArgs a, const float2 *__restrict__ stw, float2 *gbuf0, float2 *gbuf1, int cur0, int iters,
+                   int keep_gp) {
+  constexpr int T = N / 16;
+  constexpr int P = N + N / 16;
+  constexpr int W = proj_words(N);
+  extern __shared__ __align__(16) float2 sm[];
+  float2 *tw_s = sm;
+  float2 *Xs = sm + N;
+  const size_t off = (size_t)blockIdx.x * N * N;
+  const uint8_t *flags = a.flags + off;
+  float2 *Xg = a.dst + off;
+  stage_twiddles<N>(tw_s, stw);
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) Xs[(i / N) * P + (i % N)] = Xg[i];
+  cp_async_wait_all();
+  __syncthreads();
+  int cur = cur0;
+  for (int it = 0; it < iters; it++) {
+    cur ^= 1;
+    const float2 *g0 = (cur ? gbuf0 : gbuf1) + off;  // the previous model
+    float2 *g1 = (cur ? gbuf1 : gbuf0) + off;        // the new one
+    const float beta = a.alg == ALG_ER ? 0.0f : (a.beta_tab ? a.beta_tab[*a.beta_base + it] : a.beta);
+    const float one_m2b = fsub(1.0f, fmul(2.0f, beta));
+    {  // column pass: column c, thread t of its T
+      const int c = threadIdx.x % N, t = threadIdx.x / N;
+      float2 v[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] = Xs[(t + T * q) * P + c];
+      __syncthreads();  // every column read before its elements serve as exchange space
+      reg::PStages<N, 0, 1, false, P>::run(v, Xs + c, t, tw_s);
+      project16<T, true>(v, a.amp_line + (size_t)c * N, a.meas_bits + (size_t)c * W, t, (size_t)t * N + c,
+                         (size_t)T * N, a);
+      reg::PStages<N, 0, 1, true, P>::run(v, Xs + c, t, tw_s);
+#pragma unroll
+      for (int q = 0; q < 16; q++) Xs[(t + T * q) * P + c] = v[q];
+      __syncthreads();
+    }
+    {  // row pass: row r, thread t of its T
+      const int r = threadIdx.x / T, t = threadIdx.x % T;
+      float2 v[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] = Xs[r * P + t + T * q];
+      __syncthreads();  // every row read before its slots serve as exchange space
+      reg::PStages<N, 0, 1, true, 0>::run(v, Xs + r * P, t, tw_s);
+      const bool last = keep_gp && it == iters - 1;
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const int idx = r * N + t + T * q;
+        const float2 gpv = scale_cmul_dev(v[q], a.inv_n);
+        if (last) a.gp[off + idx] = gpv;
+        const uint8_t f = flags[idx];
+        float2 g = make_float2(0.0f, 0.0f);
+        if (f & FLAG_INSIDE) {
+          g = gpv;
+        } else if (a.alg == ALG_HIO) {
+          const float2 o = g0[idx];
+          g = make_float2(fsub(o.x, fmul(gpv.x, beta)), fsub(o.y, fmul(gpv.y, beta)));
+        } else if (a.alg == ALG_RAAR) {
+          const float2 o = g0[idx];
+          g = make_float2(fadd(fmul(gpv.x, one_m2b), fmul(o.x, beta)), fadd(fmul(gpv.y, one_m2b), fmul(o.y, beta)));
+        }
+        g = apply_constraints(g, f, a.constraints);
+        g1[idx] = g;
+        v[q] = g;
+      }
+      reg::PStages<N, 0, 1, false, 0>::run(v, Xs + r * P, t, tw_s);
+#pragma unroll
+      for (int q = 0; q < 16; q++) Xs[r * P + t + T * q] = v[q];
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) Xg[i] = Xs[(i / N) * P + (i % N)];
+}
+
+template <int N>
+static cudaError_t persist_launch(const LinePlan &px, const PassArgs &a, float2 *g0, float2 *g1, int cur0, int iters,
+                                  int keep_gp, int nb, cudaStream_t st) {
+  const size_t smem = (size_t)(N + N * (N + N / 16)) * sizeof(float2);
+  cudaError_t e = ensure_smem<persist_kernel<N>>(smem);
+  if (e != cudaSuccess) return e;
+  persist_kernel<N><<<nb, N * N / 16, smem, st>>>(a, px.stw, g0, g1, cur0, iters, keep_gp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_persist(const LinePlan &px, const PassArgs &a, float2 *g0, float2 *g1, int cur0, int iters,
+                           int keep_gp, int nb, cudaStream_t st) {
+  if (!px.stw || a.meas_words != proj_words(px.n)) return cudaErrorNotSupported;
+  switch (px.n) {
+    case 32: return persist_launch<32>(px, a, g0, g1, cur0, iters, keep_gp, nb, st);
+    case 64: return persist_launch<64>(px, a, g0, g1, cur0, iters, keep_gp, nb, st);
+    case 128: return persist_launch<128>(px, a, g0, g1, cur0, iters, keep_gp, nb, st);
+  }
+  return cudaErrorNotSupported;
+}
+
 // ------------------------------------------- self-check of the roundings
 // Bit-for-bit comparisons of the branch-free forms with the IEEE intrinsics,
 // counting differences: every float x with bit pattern in [lo, hi) inside the

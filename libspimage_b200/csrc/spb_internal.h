@@ -113,6 +113,11 @@ struct SelectState {
 // line length or mode has none
 cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
+// all iterations of a call for every start of an N x N pattern (N = 32, 64,
+// 128), one block per start with its spectrum resident (spb_fast.cu); a.dst
+// holds X on entry and exit, g0/g1 are the two iterate buffers (start-major)
+cudaError_t launch_persist(const LinePlan &px, const PassArgs &a, float2 *g0, float2 *g1, int cur0, int iters,
+                           int keep_gp, int nb, cudaStream_t st);
 // 8-point kernels of the iteration's two passes (spb_split.cu)
 cudaError_t launch_row_split(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col_split(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);

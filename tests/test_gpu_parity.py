@@ -215,11 +215,11 @@ def test_autotune_and_launch_shapes_leave_results_unchanged(lib, oracle_mod, sha
     assert tuned.iterate(7) == 0 and ref.iterate(7) == 0
     choice = tuned.autotune()
     assert choice["row_lines"] >= 0 and choice["no_pdl"] in (0, 1) and choice["row_g0"] in (1, 2)
-    assert choice["split"] in (1, 2)
+    assert choice["split"] in (1, 2) and choice["persist"] in (1, 2)
     assert tuned.autotune() == choice  # cached
     assert tuned.iterate(45) == 0 and ref.iterate(45) == 0
     _compare(tuned, ref)
-    for knob, value in ((0, 1), (0, 2), (1, 1), (2, 1), (2, 2), (3, 1), (3, 2)):
+    for knob, value in ((0, 1), (0, 2), (1, 1), (2, 1), (2, 2), (3, 1), (3, 2), (4, 1), (4, 2)):
         other = setup(lib.Phaser(shape), shape, alg, sup)
         other.set_tuning(knob, value)
         assert other.iterate(52) == 0

@@ -199,3 +199,43 @@ def test_plain_hio_256_full_trajectory(lib, oracle_mod):
     traj_g, traj_r = np.array(traj_g), np.array(traj_r)
     assert np.all(np.abs(traj_g - traj_r) <= 1e-3 * traj_r), np.max(np.abs(traj_g - traj_r) / traj_r)
     assert_same_state(gpu, ref)
+
+
+PERSIST = 4  # tuning knob: 2 = all iterations of a call in one launch, spectra resident per start
+
+
+@pytest.mark.parametrize("shape,alg,sup,cons", [
+    ((32, 32), HIO, [(AREA, 7, 2.0, 0.1)], 2),
+    ((64, 64), RAAR, [(AREA, 20, {0: 3.0, 200: 0.7}, 0.05)], 2),
+    ((128, 128), HIO, [(AREA, 20, {0: 3.0, 200: 0.7}, 0.05)], 2),
+    ((128, 128), ER, [(AREA, 9, 2.0, 0.1)], 1 | 16),
+    ((64, 64), HIO, None, 4 | 8),
+])
+def test_persistent_small_patterns_bit_exact(lib, oracle_mod, shape, alg, sup, cons):
+    """The persistent form (one launch per call, one block per start with its
+    spectrum in shared memory) against the oracle: calls of many lengths,
+    support updates between them, every constraint family."""
+    pat = synth.make_pattern(shape, shape[0] // 4, 1e7, shape[0] / 32.0, seed=4)
+    ref = setup_pattern(oracle_mod.Restatement(shape), pat, alg, 0.9, sup, constraints=cons, seed=6)
+    gpu = setup_pattern(lib.Phaser(shape), pat, alg, 0.9, sup, constraints=cons, seed=6)
+    gpu.set_tuning(PERSIST, 2)
+    for n in (1, 2, 19, 64, 70, 31):
+        assert ref.iterate(n) == 0 and gpu.iterate(n) == 0
+        assert same_bits(gpu.model(), ref.model()), f"after {gpu.iteration} slots"
+    assert_same_state(gpu, ref)
+
+
+@pytest.mark.parametrize("shape", [(64, 64), (128, 128)])
+def test_persistent_batch_bit_exact(lib, oracle_mod, shape):
+    """A batch of starts in the persistent form: one block per start; starts
+    0 and last against oracle runs of their seeds."""
+    pat = synth.make_pattern(shape, shape[0] // 4, 1e7, shape[0] / 32.0, seed=2)
+    sup = [(AREA, 20, {0: 3.0, 400: 0.7}, 0.05)]
+    seeds = list(range(20, 20 + 150))
+    gpu = setup_pattern(lib.Phaser(shape), pat, HIO, 0.9, sup, starts=seeds)
+    gpu.set_tuning(PERSIST, 2)
+    assert gpu.iterate(61) == 0
+    for k in (0, len(seeds) - 1):
+        ref = setup_pattern(oracle_mod.Restatement(shape), pat, HIO, 0.9, sup, seed=seeds[k])
+        assert ref.iterate(61) == 0
+        assert_same_state(gpu, ref, start=k)
