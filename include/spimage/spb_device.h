@@ -89,7 +89,8 @@ const char *spb_kernel_name(int kind);
  * iterations of a call of a 32x32, 64x64 or 128x128 pattern (HIO, RAAR or
  * ER; modulus projection without error margins) in one launch, one block per
  * start holding its spectrum in shared memory, 1 = the two-pass kernels,
- * 0 the built-in choice.  Setting a knob drops the context's captured
+ * 0 the built-in choice (persistent for 32x32 and 64x64 patterns with at
+ * least one start per SM).  Setting a knob drops the context's captured
  * graphs. */
 enum {
   SPB_TUNE_ROW_LINES = 0,

@@ -949,10 +949,17 @@ static bool persist_wanted_shape(const spb_ctx *c, const spb_alg_desc *alg) {
 }
 
 // The built-in choice between the persistent and the two-pass forms of a
-// supported pattern (measured on one B200; see persist_wanted).
+// supported pattern: persistent for 32x32 and 64x64 patterns with at least
+// one start per SM.  Measured on one B200 (HIO, calls of 20 iterations and an
+// area update between them), start-iterations/s persistent / two-pass:
+// 32x32 x 148 and 592 starts 1.46 and 1.30; 64x64 x 148, 296, 592 starts
+// 1.11, 1.12, 1.27 but x 1 and 8 starts 0.84, 0.89 (one SM per start);
+// 128x128 x 148 and 296 starts 0.99 (both forms at the same issue-bound
+// pixel rate) and x 1, 8 starts 0.39, 0.40.
 static bool persist_auto(const spb_ctx *c) {
-  (void)c;
-  return false;
+  static int nsm = 0;
+  if (!nsm && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) nsm = 148;
+  return c->nx <= 64 && c->nb >= nsm;
 }
 
 // One iteration of every start: g0 <- g1 (buffer roles swap), X -> Y
