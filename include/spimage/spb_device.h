@@ -90,15 +90,18 @@ const char *spb_kernel_name(int kind);
  * ER; modulus projection without error margins) in one launch, one block per
  * start holding its spectrum in shared memory, 1 = the two-pass kernels,
  * 0 the built-in choice (persistent for 32x32 and 64x64 patterns with at
- * least one start per SM).  Setting a knob drops the context's captured
- * graphs. */
+ * least one start per SM); SPB_TUNE_COL_WIDTH = columns per block of the
+ * projection pass along the last axis, for lines of 256 (1..16 columns),
+ * 512 (1..8) or 1024 (1..4) points; 0 the built-in width.  Setting a knob
+ * drops the context's captured graphs. */
 enum {
   SPB_TUNE_ROW_LINES = 0,
   SPB_TUNE_NO_PDL = 1,
   SPB_TUNE_ROW_G0 = 2,
   SPB_TUNE_SPLIT = 3,
   SPB_TUNE_PERSIST = 4,
-  SPB_TUNE_KNOBS = 5
+  SPB_TUNE_COL_WIDTH = 5,
+  SPB_TUNE_KNOBS = 6
 };
 int spb_ctx_set_tuning(spb_ctx *ctx, int knob, int value);
 int spb_ctx_get_tuning(spb_ctx *ctx, int knob);

@@ -501,7 +501,7 @@ class Phaser:
         ctx = self.lib.sp_phaser_device_context(self.ph)
         return {"row_lines": self.lib.spb_ctx_get_tuning(ctx, 0), "no_pdl": self.lib.spb_ctx_get_tuning(ctx, 1),
                 "row_g0": self.lib.spb_ctx_get_tuning(ctx, 2), "split": self.lib.spb_ctx_get_tuning(ctx, 3),
-                "persist": self.lib.spb_ctx_get_tuning(ctx, 4)}
+                "persist": self.lib.spb_ctx_get_tuning(ctx, 4), "col_width": self.lib.spb_ctx_get_tuning(ctx, 5)}
 
     def set_tuning(self, knob, value):
         ctx = self.lib.sp_phaser_device_context(self.ph)

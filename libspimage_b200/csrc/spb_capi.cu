@@ -257,6 +257,7 @@ PassArgs base_args(const spb_ctx *c) {
   a.row_g0 = c->tune[SPB_TUNE_ROW_G0];
   a.pdl = c->tune[SPB_TUNE_NO_PDL] ? 0 : 1;
   a.split = c->tune[SPB_TUNE_SPLIT];
+  a.col_width = c->tune[SPB_TUNE_COL_WIDTH];
   a.inv_n = (float)(1.0 / (double)c->n);
   a.nx_f = (float)c->nx;
   a.n_f = (float)c->n;
@@ -558,6 +559,9 @@ static void drop_graphs(spb_ctx *c) {
 
 extern "C" int spb_ctx_set_tuning(spb_ctx *c, int knob, int value) {
   if (knob < 0 || knob >= SPB_TUNE_KNOBS) return fail("unknown tuning knob %d", knob);
+  if (knob == SPB_TUNE_COL_WIDTH && value != 0 && !col_width_ok(c->nz > 1 ? c->nz : c->ny, value))
+    return fail("no projection pass of %d columns per block for lines of %d points", value,
+                c->nz > 1 ? c->nz : c->ny);
   if (value < 0) return fail("negative tuning value %d", value);
   if (c->tune[knob] != value) {
     c->tune[knob] = value;
@@ -1461,14 +1465,14 @@ struct TuneKey {
 };
 std::mutex g_tune_mu;
 struct TuneChoice {
-  int lines, nopdl, g0, split, persist;
+  int lines, nopdl, g0, split, persist, colw;
 };
 std::map<TuneKey, TuneChoice> g_tune_cache;
 
 int apply_choice(spb_ctx *c, const TuneChoice &t) {
   if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, t.lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, t.nopdl) ||
       spb_ctx_set_tuning(c, SPB_TUNE_ROW_G0, t.g0) || spb_ctx_set_tuning(c, SPB_TUNE_SPLIT, t.split) ||
-      spb_ctx_set_tuning(c, SPB_TUNE_PERSIST, t.persist))
+      spb_ctx_set_tuning(c, SPB_TUNE_PERSIST, t.persist) || spb_ctx_set_tuning(c, SPB_TUNE_COL_WIDTH, t.colw))
     return -1;
   return 0;
 }
@@ -1500,7 +1504,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   const int cur0 = c->cur, xv0 = c->x_valid, xfv0 = c->xf_valid;
   const float xfg0 = c->xf_gamma1;
   const TuneChoice knob0{c->tune[SPB_TUNE_ROW_LINES], c->tune[SPB_TUNE_NO_PDL], c->tune[SPB_TUNE_ROW_G0],
-                         c->tune[SPB_TUNE_SPLIT], c->tune[SPB_TUNE_PERSIST]};
+                         c->tune[SPB_TUNE_SPLIT], c->tune[SPB_TUNE_PERSIST], c->tune[SPB_TUNE_COL_WIDTH]};
   int rc = 0;
   const float2 *bufs[4] = {c->g[0], c->g[1], c->gp, c->X};
   for (int k = 0; k < 4 && !rc; k++)
@@ -1515,43 +1519,60 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   const int T = c->nx >= 16 ? c->nx / 16 : 1;
   const int lpb_max = 256 / T > 0 ? 256 / T : 1;
   double best = 1e30;
-  TuneChoice bestc{0, 0, 0, 0, 1};
+  TuneChoice bestc{0, 0, 0, 0, 1, 0};
   // 8-point kernels exist for these row (x) and projection-axis lengths
   auto split_len = [](int n) { return n == 256 || n == 512 || n == 1024 || n == 4096; };
-  const bool can_split = split_len(c->nx) || split_len(c->nz > 1 ? c->nz : c->ny);
+  const int plen = c->nz > 1 ? c->nz : c->ny;
+  const bool can_split = split_len(c->nx) || split_len(plen);
   const bool can_persist = persist_wanted_shape(c, alg);
-  // the two-pass launch shapes, then (where it applies) the persistent form,
-  // which has no launch-shape knobs of its own
-  for (int cand = 0; cand < 2 * 2 * 2 * 16 + 1 && !rc; cand++) {
-    const bool pcand = cand == 2 * 2 * 2 * 16;
-    if (pcand && !can_persist) continue;
-    const int nopdl = pcand ? 0 : cand & 1, g0 = pcand ? 1 : 1 + ((cand >> 1) & 1);
-    const int sp = pcand ? 1 : 1 + ((cand >> 2) & 1), li = pcand ? 0 : cand >> 3;
+  // time one candidate: the model, iterates and support are restored after the search
+  auto time_choice = [&](const TuneChoice &t) {
+    if (apply_choice(c, t)) {
+      rc = -1;
+      return;
+    }
+    // warm-up: a direct call, then the graph capture
+    for (int w = 0; w < 2 && !rc; w++) rc = spb_ctx_iterate(c, alg, beta.data(), iterations, 1);
+    if (rc) return;
+    if (cudaEventRecord(e0, c->st) != cudaSuccess) rc = fail("autotune: event");
+    for (int k = 0; k < calls && !rc; k++) rc = spb_ctx_iterate(c, alg, beta.data(), iterations, 1);
+    if (!rc && cudaEventRecord(e1, c->st) != cudaSuccess) rc = fail("autotune: event");
+    float ms = 0.0f;
+    if (!rc && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+      rc = fail("autotune: timing failed");
+    if (!rc && ms < best) {
+      best = ms;
+      bestc = t;
+    }
+  };
+  // 1. the two-pass launch shapes: row lines per block x dependent launch x
+  //    g0 staging, and the 8-point passes (one block shape of their own)
+  std::vector<TuneChoice> cands;
+  for (int li = 0; li < 16; li++) {
     const int lines = li ? 1 << (li - 1) : 0;
     if (lines > lpb_max) continue;  // (0 is the built-in choice, which may be lpb_max or fewer)
-    // the 8-point row kernel has one block shape: no lines-per-block candidates
-    if (sp == 2 && (!can_split || li != 0)) continue;
-    const int pe = pcand ? 2 : 1;
-    {
-      if (apply_choice(c, TuneChoice{lines, nopdl, g0, sp, pe})) {
-        rc = -1;
-        break;
-      }
-      // warm-up: a direct call, then the graph capture
-      for (int w = 0; w < 2 && !rc; w++) rc = spb_ctx_iterate(c, alg, beta.data(), iterations, 1);
-      if (rc) break;
-      if (cudaEventRecord(e0, c->st) != cudaSuccess) rc = fail("autotune: event");
-      for (int k = 0; k < calls && !rc; k++) rc = spb_ctx_iterate(c, alg, beta.data(), iterations, 1);
-      if (!rc && cudaEventRecord(e1, c->st) != cudaSuccess) rc = fail("autotune: event");
-      float ms = 0.0f;
-      if (!rc && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
-        rc = fail("autotune: timing failed");
-      if (!rc && ms < best) {
-        best = ms;
-        bestc = TuneChoice{lines, nopdl, g0, sp, pe};
-      }
+    for (int sp = 1; sp <= 2; sp++) {
+      if (sp == 2 && (!can_split || li != 0)) continue;
+      for (int g0 = 1; g0 <= 2; g0++)
+        for (int nopdl = 0; nopdl <= 1; nopdl++) cands.push_back(TuneChoice{lines, nopdl, g0, sp, 1, 0});
     }
   }
+  for (const TuneChoice &t : cands) {
+    if (rc) break;
+    time_choice(t);
+  }
+  // 2. with the best of those, the projection pass's columns per block
+  if (!rc && bestc.split == 1) {
+    const TuneChoice base = bestc;
+    for (int w = 1; w <= 16 && !rc; w <<= 1)
+      if (col_width_ok(plen, w)) {
+        TuneChoice t = base;
+        t.colw = w;
+        time_choice(t);
+      }
+  }
+  // 3. the persistent form, where it applies (no launch-shape knobs)
+  if (!rc && can_persist) time_choice(TuneChoice{0, 0, 1, 1, 2, 0});
   // restore the state and apply the choice (or the previous knobs on error)
   for (int k = 0; k < 4; k++)
     cudaMemcpyAsync((void *)bufs[k], save + (size_t)k * c->ntot, nc, cudaMemcpyDeviceToDevice, c->st);

@@ -768,9 +768,8 @@ __host__ __device__ static constexpr int col_width() {
   return N >= 2048 ? (4096 / N) : (N >= 512 ? 4 : (N >= 256 ? 8 : 16));
 }
 
-template <int N, int MODE, bool PREFETCH>
+template <int N, int MODE, bool PREFETCH, int C = col_width<N>()>
 static cudaError_t col_fast_launch_p(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
-  constexpr int C = col_width<N>();
   constexpr int T = N / 16;
   size_t smem = (size_t)(N + C * (N + N / 16 + (C > 1 ? 16 / C : 0))) * sizeof(float2);
   if (PREFETCH) {
@@ -788,13 +787,34 @@ static cudaError_t col_fast_launch_p(const LinePlan &pl, const PassArgs &a, cuda
   return launch_maybe_pdl(k, grid, dim3(C * T), smem, st, a.pdl != 0, a, pl.stw);
 }
 
+// Columns per block the projection pass offers besides the built-in width:
+// lines of 256, 512 and 1024 points, C a power of two with C*N/16 <= 256
+// threads and C <= 16 (the shared-memory skew is 16/C words).
+bool col_width_ok(int n, int w) {
+  if (w < 1 || w > 16 || (w & (w - 1))) return false;
+  if (n != 256 && n != 512 && n != 1024) return false;
+  return w * (n / 16) <= 256;
+}
+
 template <int N, int MODE>
 static cudaError_t col_fast_launch(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
   constexpr bool PROJ = (MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC);
   // projection passes run along the last axis; every start (outer index)
   // shares the line-major amplitude and measured-bit lines of its column
-  if (PROJ && a.amp_line && a.meas_bits && (a.meas_words % 4) == 0)
+  if (PROJ && a.amp_line && a.meas_bits && (a.meas_words % 4) == 0) {
+    if constexpr (PROJ && (N == 256 || N == 512 || N == 1024)) {
+      // a launch-shape knob: another number of columns per block
+      switch (a.col_width) {
+        case 1: return col_fast_launch_p<N, MODE, true, 1>(pl, a, st);
+        case 2: return col_fast_launch_p<N, MODE, true, 2>(pl, a, st);
+        case 4: return col_fast_launch_p<N, MODE, true, 4>(pl, a, st);
+        case 8: if constexpr (8 * (N / 16) <= 256) return col_fast_launch_p<N, MODE, true, 8>(pl, a, st); break;
+        case 16: if constexpr (16 * (N / 16) <= 256) return col_fast_launch_p<N, MODE, true, 16>(pl, a, st); break;
+        default: break;
+      }
+    }
     return col_fast_launch_p<N, MODE, PROJ>(pl, a, st);
+  }
   return col_fast_launch_p<N, MODE, false>(pl, a, st);
 }
 

@@ -77,6 +77,8 @@ struct PassArgs {
   // (when the 16-point kernels would leave the SMs short of warps), 1 never,
   // 2 wherever a kernel exists
   int split;
+  // columns per block of the projection pass (0: the built-in width); see col_width_ok
+  int col_width;
   // 1: launch the register pass kernels with programmatic dependent launch
   int pdl;
   // scalars
@@ -113,6 +115,8 @@ struct SelectState {
 // line length or mode has none
 cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
+// whether the projection pass has a kernel of w columns per block for lines of n points
+bool col_width_ok(int n, int w);
 // all iterations of a call for every start of an N x N pattern (N = 32, 64,
 // 128), one block per start with its spectrum resident (spb_fast.cu); a.dst
 // holds X on entry and exit, g0/g1 are the two iterate buffers (start-major)

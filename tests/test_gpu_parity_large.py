@@ -239,3 +239,25 @@ def test_persistent_batch_bit_exact(lib, oracle_mod, shape):
         ref = setup_pattern(oracle_mod.Restatement(shape), pat, HIO, 0.9, sup, seed=seeds[k])
         assert ref.iterate(61) == 0
         assert_same_state(gpu, ref, start=k)
+
+
+COL_WIDTH = 5  # tuning knob: columns per block of the projection pass
+
+
+@pytest.mark.parametrize("shape,widths", [((256, 64), (1, 2, 4, 8, 16)), ((512, 96), (1, 2, 4, 8)),
+                                          ((1024, 32), (1, 2, 4))])
+def test_projection_column_widths_bit_exact(lib, oracle_mod, shape, widths):
+    """Every columns-per-block shape of the projection pass the autotuner can
+    choose gives the oracle's bits."""
+    pat = synth.make_pattern(shape, min(shape) // 4, 1e7, min(shape) / 32.0, seed=8)
+    sup = [(AREA, 9, 2.0, 0.1)]
+    ref = setup_pattern(oracle_mod.Restatement(shape, threads=8), pat, RAAR, 0.87, sup, seed=3)
+    assert ref.iterate(23) == 0
+    for w in widths:
+        gpu = setup_pattern(lib.Phaser(shape), pat, RAAR, 0.87, sup, seed=3)
+        gpu.set_tuning(SPLIT, 1)
+        gpu.set_tuning(COL_WIDTH, w)
+        assert gpu.iterate(23) == 0
+        assert same_bits(gpu.model(), ref.model()), f"{w} columns per block"
+    with pytest.raises(RuntimeError, match="columns per block"):
+        gpu.set_tuning(COL_WIDTH, 3)
