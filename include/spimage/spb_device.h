@@ -92,8 +92,11 @@ const char *spb_kernel_name(int kind);
  * 0 the built-in choice (persistent for 32x32 and 64x64 patterns with at
  * least one start per SM); SPB_TUNE_COL_WIDTH = columns per block of the
  * projection pass along the last axis, for lines of 256 (1..16 columns),
- * 512 (1..8) or 1024 (1..4) points; 0 the built-in width.  Setting a knob
- * drops the context's captured graphs. */
+ * 512 (1..8) or 1024 (1..4) points; 0 the built-in width; SPB_TUNE_TMA = 2
+ * stages the projection pass's column tiles with the tensor memory
+ * accelerator (bulk tensor loads under an mbarrier and bulk tensor stores),
+ * 1 or 0 with plain loads and stores.  Setting a knob drops the context's
+ * captured graphs. */
 enum {
   SPB_TUNE_ROW_LINES = 0,
   SPB_TUNE_NO_PDL = 1,
@@ -101,7 +104,8 @@ enum {
   SPB_TUNE_SPLIT = 3,
   SPB_TUNE_PERSIST = 4,
   SPB_TUNE_COL_WIDTH = 5,
-  SPB_TUNE_KNOBS = 6
+  SPB_TUNE_TMA = 6,
+  SPB_TUNE_KNOBS = 7
 };
 int spb_ctx_set_tuning(spb_ctx *ctx, int knob, int value);
 int spb_ctx_get_tuning(spb_ctx *ctx, int knob);

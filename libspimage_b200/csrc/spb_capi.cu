@@ -228,6 +228,7 @@ struct spb_ctx {
   SelectState *sel = nullptr;  // one per start
   double *red = nullptr;       // reduce_scratch_doubles(nb)
   unsigned *nonfinite = nullptr;  // sticky flag of spb_ctx_nonfinite_async
+  int *err_flag = nullptr;        // set by a kernel whose bounded wait ran out
   unsigned long long *seeds = nullptr;  // per-start generator keys (device starts)
   int x_valid = 0, xf_valid = 0;
   float xf_gamma1 = 0.0f;
@@ -258,6 +259,8 @@ PassArgs base_args(const spb_ctx *c) {
   a.pdl = c->tune[SPB_TUNE_NO_PDL] ? 0 : 1;
   a.split = c->tune[SPB_TUNE_SPLIT];
   a.col_width = c->tune[SPB_TUNE_COL_WIDTH];
+  a.tma = c->tune[SPB_TUNE_TMA];
+  a.err_flag = c->err_flag;
   a.inv_n = (float)(1.0 / (double)c->n);
   a.nx_f = (float)c->nx;
   a.n_f = (float)c->n;
@@ -494,6 +497,8 @@ extern "C" int spb_ctx_create_batch(spb_ctx **out, int nx, int ny, int nz, int n
   alloc((void **)&c->sel, sizeof(SelectState) * (size_t)nb);
   alloc((void **)&c->red, sizeof(double) * (size_t)reduce_scratch_doubles(nb));
   alloc((void **)&c->nonfinite, sizeof(unsigned));
+  alloc((void **)&c->err_flag, sizeof(int));
+  if (!rc && cudaMemsetAsync(c->err_flag, 0, sizeof(int), c->st) != cudaSuccess) rc = fail("cudaMemsetAsync");
   alloc((void **)&c->seeds, sizeof(unsigned long long) * (size_t)nb);
   alloc((void **)&c->beta_zero, sizeof(int));
   alloc((void **)&c->spar, sizeof(SupportParams));
@@ -599,7 +604,8 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
-                  c->gp, c->T, c->absb, c->gtab, c->sel, c->red, c->nonfinite, c->ax.tw, c->ay.tw, c->az.tw,
+                  c->gp, c->T, c->absb, c->gtab, c->sel, c->red, c->nonfinite, c->err_flag, c->ax.tw, c->ay.tw,
+                  c->az.tw,
                   c->amp_line, c->amp_bad, c->meas_bits, c->beta_dev, c->beta_base, c->seeds, c->beta_zero, c->spar};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -619,9 +625,10 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   delete c;
 }
 
+static int check_err_flag(spb_ctx *c);
 extern "C" int spb_ctx_synchronize(spb_ctx *c) {
   CK(cudaStreamSynchronize(c->st));
-  return 0;
+  return check_err_flag(c);
 }
 
 static const char *kKernelNames[SPB_KERNEL_KINDS] = {
@@ -675,10 +682,21 @@ static int upload(spb_ctx *c, void *dst, const void *src, size_t bytes) {
   return 0;
 }
 
+// after the context's stream has drained: a kernel whose bounded wait ran
+// out (a tile that never arrived) has set the error flag
+static int check_err_flag(spb_ctx *c) {
+  if (!c->tune[SPB_TUNE_TMA]) return 0;
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->err_flag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (h) return fail("a pass kernel gave up waiting for its tile (bounded mbarrier wait): results are invalid");
+  return 0;
+}
+
 static int download(spb_ctx *c, void *dst, const void *src, size_t bytes) {
   CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  return 0;
+  return check_err_flag(c);
 }
 
 namespace spb {

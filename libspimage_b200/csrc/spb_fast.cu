@@ -18,6 +18,8 @@
 // lines per row: inverse x of Y and Yf, the update, forward x of g and f1).
 // Column kernels: transforms, the Fourier projection with line-major
 // amplitudes and measured bits, the blur multiplier.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <math.h>
 
 #include "spb_internal.h"
@@ -477,6 +479,187 @@ __global__ void __launch_bounds__(256) col_fast_kernel(PassArgs a, const float2 
     for (int q = 0; q < 16; q++) a.dst[lbase + q * qstride] = v[q];
 }
 
+// --------------------------------------- projection pass staged by TMA
+// The column projection pass with its column tile moved by the tensor memory
+// accelerator: one thread issues cp.async.bulk.tensor loads of the block's C
+// columns (N rows, boxes of up to 256 rows) into shared memory under an
+// mbarrier, the threads read their natural-layout points from the dense tile,
+// and after the inverse transform the tile is written back to shared memory
+// and stored by cp.async.bulk.tensor.  The tile lives in the exchange lines'
+// space, which is free before the first stage and after the last.  The
+// tensor maps cover only this GPU's memory (the iterate buffers of the
+// context) and no load uses cluster multicast.  Transforms, projection and
+// bits are those of col_fast_kernel.
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"((unsigned long long)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, int x, int y, const void *src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                   (unsigned long long)map),
+               "r"(x), "r"(y), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// polls of the tile's mbarrier before the block gives up (each try_wait may
+// suspend the thread for a while; a stuck copy ends the block within seconds)
+constexpr long long kTmaWaitPolls = 1LL << 22;
+
+template <int N, int MODE, int C>
+__global__ void __launch_bounds__(256) col_tma_kernel(PassArgs a, const float2 *__restrict__ stw,
+                                                      const __grid_constant__ CUtensorMap tin,
+                                                      const __grid_constant__ CUtensorMap tout) {
+  constexpr int T = N / 16;
+  constexpr int S = N + N / 16 + (C > 1 ? 16 / C : 0);
+  constexpr int BOX = N < 256 ? N : 256;
+  static_assert(C * S >= C * N, "the tile fits the exchange lines");
+  extern __shared__ __align__(128) float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
+  const int c = threadIdx.x % C, t = threadIdx.x / C;
+  const int col0 = blockIdx.x * C;
+  float2 *tw_s = sm;
+  float2 *tile = sm + N;  // [N][C] dense, in the exchange lines' space
+  float2 *line = sm + N + c * S;
+  constexpr int W = proj_words(N);
+  constexpr int SA = amp_stride<N, C>();
+  constexpr int SW = bits_stride<N, C>();
+  float *amp_s = reinterpret_cast<float *>(sm + N + C * S);
+  uint32_t *meas_s = reinterpret_cast<uint32_t *>(amp_s + C * SA);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  stage_twiddles<N>(tw_s, stw);
+  {
+    const float *asrc = a.amp_line + (size_t)col0 * N;
+    for (int k = threadIdx.x; k < C * (N / 4); k += blockDim.x) {
+      const int l = k / (N / 4), j = k % (N / 4);
+      cp_async16(amp_s + l * SA + 4 * j, asrc + (size_t)l * N + 4 * j);
+    }
+    const uint32_t *msrc = a.meas_bits + (size_t)col0 * W;
+    for (int k = threadIdx.x; k < C * (W / 4); k += blockDim.x) {
+      const int l = k / (W / 4), j = k % (W / 4);
+      cp_async16(meas_s + l * SW + 4 * j, msrc + (size_t)l * W + 4 * j);
+    }
+  }
+  __syncthreads();  // the barrier's initialisation before any wait on it
+  const long long o = a.outer0 + blockIdx.y;
+  const size_t qstride = (size_t)T * a.estride;
+  const size_t lbase = (size_t)o * a.ostride + col0 + c + (size_t)t * a.estride;
+  pdl_wait();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&bar, (unsigned)(N * C * sizeof(float2)));
+#pragma unroll
+    for (int k = 0; k < N / BOX; k++) tma_load_2d(tile + k * BOX * C, &tin, col0, (int)(o * N + k * BOX), &bar);
+  }
+  bool ok = false;
+  for (long long i = 0; i < kTmaWaitPolls && !ok; i++) ok = mbar_try_wait(&bar, 0);
+  if (!ok) {  // the tile never arrived: flag it and leave (nothing of this block is written)
+    if (a.err_flag) atomicExch(a.err_flag, 1);
+    return;
+  }
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) v[q] = tile[(t + T * q) * C + c];
+  cp_async_wait_all();
+  __syncthreads();  // every tile read (and the operand lines in) before the exchanges reuse the space
+  reg::fft<N, false>(v, line, t, tw_s);
+  project16<T, MODE == COL_PROJECT>(v, amp_s + c * SA, meas_s + c * SW, t, lbase, qstride, a);
+  reg::fft<N, true>(v, line, t, tw_s);
+  __syncthreads();  // the exchange lines are free again
+#pragma unroll
+  for (int q = 0; q < 16; q++) tile[(t + T * q) * C + c] = v[q];
+  fence_proxy_async_smem();  // the tile's writes visible to the tensor copies
+  __syncthreads();
+  pdl_release();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < N / BOX; k++) tma_store_2d(&tout, col0, (int)(o * N + k * BOX), tile + k * BOX * C);
+    bulk_commit();
+    bulk_wait_read0();  // the shared-memory tile stays until the copies have read it
+  }
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// a 2-D view of a buffer of float2: rows of `inner` elements (the column
+// stride), `rows` rows; boxes of C elements by `box_rows` rows
+static bool make_tile_map(CUtensorMap *m, const void *base, long long inner, long long rows, int C, int box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)inner * sizeof(float2)};
+  const cuuint32_t box[2] = {(cuuint32_t)C, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<void *>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Whether the TMA form serves this projection launch: 16-byte-aligned tile
+// columns (C >= 2 columns of 8 bytes, an even column stride), whole tiles
+// (ncols a multiple of C), lines of the tile's length, 16-byte-aligned bases.
+template <int N, int C>
+static bool tma_fits(const PassArgs &a) {
+  if (C < 2 || a.ncols % C != 0 || (a.estride & 1) || a.ostride != (long long)N * a.estride) return false;
+  if (((uintptr_t)a.src & 15) || ((uintptr_t)a.dst & 15)) return false;
+  return a.amp_line && a.meas_bits && a.meas_words == proj_words(N);
+}
+
+template <int N, int MODE, int C>
+static cudaError_t col_tma_launch(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+  constexpr int T = N / 16;
+  const size_t smem = (size_t)(N + C * (N + N / 16 + (C > 1 ? 16 / C : 0))) * sizeof(float2) +
+                      (size_t)C * amp_stride<N, C>() * sizeof(float) + (size_t)C * bits_stride<N, C>() * sizeof(uint32_t);
+  CUtensorMap tin, tout;
+  const long long rows = (a.outer0 + a.nouter) * (long long)N;
+  constexpr int BOX = N < 256 ? N : 256;
+  if (!make_tile_map(&tin, a.src, a.estride, rows, C, BOX) || !make_tile_map(&tout, a.dst, a.estride, rows, C, BOX))
+    return cudaErrorNotSupported;
+  cudaError_t e = ensure_smem<col_tma_kernel<N, MODE, C>>(smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.ncols + C - 1) / C, a.nouter);
+  return launch_maybe_pdl(col_tma_kernel<N, MODE, C>, grid, dim3(C * T), smem, st, a.pdl != 0, a, pl.stw, tin, tout);
+}
+
 // ------------------------------------------------ persistent small patterns
 // One block per start of an N x N pattern (N = 32, 64, 128) runs every
 // iteration of a call with the start's spectrum resident in shared memory:
@@ -802,6 +985,14 @@ static cudaError_t col_fast_launch(const LinePlan &pl, const PassArgs &a, cudaSt
   // projection passes run along the last axis; every start (outer index)
   // shares the line-major amplitude and measured-bit lines of its column
   if (PROJ && a.amp_line && a.meas_bits && (a.meas_words % 4) == 0) {
+    if constexpr (PROJ && N >= 64) {
+      // the tile staged by the tensor memory accelerator (knob), built-in width
+      constexpr int C = col_width<N>();
+      if (a.tma == 2 && tma_fits<N, C>(a)) {
+        const cudaError_t te = col_tma_launch<N, MODE, C>(pl, a, st);
+        if (te != cudaErrorNotSupported) return te;
+      }
+    }
     if constexpr (PROJ && (N == 256 || N == 512 || N == 1024)) {
       // a launch-shape knob: another number of columns per block
       switch (a.col_width) {

@@ -79,6 +79,9 @@ struct PassArgs {
   int split;
   // columns per block of the projection pass (0: the built-in width); see col_width_ok
   int col_width;
+  // 2: stage the projection pass's column tiles by TMA (spb_fast.cu col_tma_kernel)
+  int tma;
+  int *err_flag;  // set to 1 by a kernel whose bounded wait ran out (device)
   // 1: launch the register pass kernels with programmatic dependent launch
   int pdl;
   // scalars

@@ -261,3 +261,25 @@ def test_projection_column_widths_bit_exact(lib, oracle_mod, shape, widths):
         assert same_bits(gpu.model(), ref.model()), f"{w} columns per block"
     with pytest.raises(RuntimeError, match="columns per block"):
         gpu.set_tuning(COL_WIDTH, 3)
+
+
+TMA = 6  # tuning knob: 2 = projection pass column tiles staged by the tensor memory accelerator
+
+
+@pytest.mark.parametrize("shape,alg,starts", [((512, 512), HIO, 8), ((1024, 1024), RAAR, None), ((256, 256), DIFFMAP, None),
+                                              ((64, 64, 64), HIO, 2), ((128, 128), ER, 3), ((64, 1008), RAAR, None)])
+def test_tma_projection_bit_exact(lib, oracle_mod, shape, alg, starts):
+    """The projection pass with its column tiles moved by bulk tensor copies
+    (TMA) gives the oracle's bits: 2-D y lines, 3-D z lines (tile rows of
+    64*64 points), and 64-point columns of 1008-point rows."""
+    pat = synth.make_pattern(shape, min(shape) // 4, 1e7, min(shape) / 32.0, seed=9)
+    sup = [(AREA, 9, {0: 3.0, 60: 0.7}, 0.05)]
+    seeds = list(range(30, 30 + starts)) if starts else None
+    gpu = setup_pattern(lib.Phaser(shape), pat, alg, 0.87, sup, seed=30, starts=seeds)
+    gpu.set_tuning(TMA, 2)
+    gpu.set_tuning(PERSIST, 1)
+    assert gpu.iterate(23) == 0
+    for k in ([0, starts - 1] if starts else [None]):
+        ref = setup_pattern(oracle_mod.Restatement(shape, threads=8), pat, alg, 0.87, sup, seed=30 + (k or 0))
+        assert ref.iterate(23) == 0
+        assert_same_state(gpu, ref, start=k)
