@@ -228,7 +228,7 @@ struct spb_ctx {
   SelectState *sel = nullptr;  // one per start
   double *red = nullptr;       // reduce_scratch_doubles(nb)
   unsigned *nonfinite = nullptr;  // sticky flag of spb_ctx_nonfinite_async
-  int *err_flag = nullptr;        // set by a kernel whose bounded wait ran out
+  int *err_flag = nullptr;        // set by a kernel that gave up (bounded wait, misaligned TMA tile)
   unsigned long long *seeds = nullptr;  // per-start generator keys (device starts)
   int x_valid = 0, xf_valid = 0;
   float xf_gamma1 = 0.0f;
@@ -689,6 +689,7 @@ static int check_err_flag(spb_ctx *c) {
   int h = 0;
   CK(cudaMemcpyAsync(&h, c->err_flag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  if (h == 2) return fail("a TMA pass kernel found its shared-memory tile or first column misaligned and copied nothing: results are invalid");
   if (h) return fail("a pass kernel gave up waiting for its tile (bounded mbarrier wait): results are invalid");
   return 0;
 }

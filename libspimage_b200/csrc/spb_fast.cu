@@ -529,6 +529,8 @@ __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.p
 // polls of the tile's mbarrier before the block gives up (each try_wait may
 // suspend the thread for a while; a stuck copy ends the block within seconds)
 constexpr long long kTmaWaitPolls = 1LL << 22;
+// shared-memory alignment of the bulk tensor copies' boxes (bytes)
+constexpr unsigned kTmaSmemAlign = 128;
 
 template <int N, int MODE, int C>
 __global__ void __launch_bounds__(256) col_tma_kernel(PassArgs a, const float2 *__restrict__ stw,
@@ -538,10 +540,25 @@ __global__ void __launch_bounds__(256) col_tma_kernel(PassArgs a, const float2 *
   constexpr int S = N + N / 16 + (C > 1 ? 16 / C : 0);
   constexpr int BOX = N < 256 ? N : 256;
   static_assert(C * S >= C * N, "the tile fits the exchange lines");
-  extern __shared__ __align__(128) float2 sm[];
+  static_assert((N * sizeof(float2)) % kTmaSmemAlign == 0 && (BOX * C * sizeof(float2)) % kTmaSmemAlign == 0,
+                "every box of the tile starts on the bulk tensor copies' shared-memory alignment");
+  // The dynamic shared memory of a kernel starts where the file's first
+  // declaration of an extern shared array says, not where a later one asks
+  // for; the block rounds its base up to the copies' alignment itself (the
+  // launch adds kTmaSmemAlign bytes for it).
+  extern __shared__ unsigned char tma_smem_raw[];
   __shared__ __align__(8) uint64_t bar;
+  float2 *sm = reinterpret_cast<float2 *>(
+      tma_smem_raw + ((kTmaSmemAlign - (smem_u32(tma_smem_raw) & (kTmaSmemAlign - 1))) & (kTmaSmemAlign - 1)));
   const int c = threadIdx.x % C, t = threadIdx.x / C;
   const int col0 = blockIdx.x * C;
+  // self-check before any copy is issued (uniform over the block): a tile
+  // that is not aligned, or a first column whose byte offset is not a
+  // multiple of 16, is reported through the error flag and nothing is copied
+  if ((smem_u32(sm + N) & (kTmaSmemAlign - 1)) || ((col0 * (int)sizeof(float2)) & 15)) {
+    if (threadIdx.x == 0 && a.err_flag) atomicExch(a.err_flag, 2);
+    return;
+  }
   float2 *tw_s = sm;
   float2 *tile = sm + N;  // [N][C] dense, in the exchange lines' space
   float2 *line = sm + N + c * S;
@@ -648,7 +665,8 @@ template <int N, int MODE, int C>
 static cudaError_t col_tma_launch(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
   constexpr int T = N / 16;
   const size_t smem = (size_t)(N + C * (N + N / 16 + (C > 1 ? 16 / C : 0))) * sizeof(float2) +
-                      (size_t)C * amp_stride<N, C>() * sizeof(float) + (size_t)C * bits_stride<N, C>() * sizeof(uint32_t);
+                      (size_t)C * amp_stride<N, C>() * sizeof(float) + (size_t)C * bits_stride<N, C>() * sizeof(uint32_t) +
+                      kTmaSmemAlign;  // room to round the block's base up to the copies' alignment
   CUtensorMap tin, tout;
   const long long rows = (a.outer0 + a.nouter) * (long long)N;
   constexpr int BOX = N < 256 ? N : 256;

@@ -81,7 +81,7 @@ struct PassArgs {
   int col_width;
   // 2: stage the projection pass's column tiles by TMA (spb_fast.cu col_tma_kernel)
   int tma;
-  int *err_flag;  // set to 1 by a kernel whose bounded wait ran out (device)
+  int *err_flag;  // set by a kernel that could not do its work (device): 1 a bounded wait ran out, 2 a misaligned TMA tile
   // 1: launch the register pass kernels with programmatic dependent launch
   int pdl;
   // scalars
