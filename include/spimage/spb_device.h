@@ -92,11 +92,13 @@ const char *spb_kernel_name(int kind);
  * 0 the built-in choice (persistent for 32x32 and 64x64 patterns with at
  * least one start per SM); SPB_TUNE_COL_WIDTH = columns per block of the
  * projection pass along the last axis, for lines of 256 (1..16 columns),
- * 512 (1..8) or 1024 (1..4) points; 0 the built-in width; SPB_TUNE_TMA = 2
- * stages the projection pass's column tiles with the tensor memory
- * accelerator (bulk tensor loads under an mbarrier and bulk tensor stores),
- * 1 or 0 with plain loads and stores.  Setting a knob drops the context's
- * captured graphs. */
+ * 512 (1..8) or 1024 (1..4) points; 0 the built-in width; SPB_TUNE_TMA:
+ * how the projection pass of 16-point lines of 64 points or more moves its
+ * column tiles -- 0 (the built-in choice) with the tensor memory accelerator
+ * (bulk tensor loads under an mbarrier and bulk tensor stores) where the
+ * tile fits and no other column width is asked for, 2 with it wherever the
+ * tile fits, 1 with plain loads and stores.  Setting a knob drops the
+ * context's captured graphs. */
 enum {
   SPB_TUNE_ROW_LINES = 0,
   SPB_TUNE_NO_PDL = 1,

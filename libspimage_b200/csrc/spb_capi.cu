@@ -685,7 +685,7 @@ static int upload(spb_ctx *c, void *dst, const void *src, size_t bytes) {
 // after the context's stream has drained: a kernel whose bounded wait ran
 // out (a tile that never arrived) has set the error flag
 static int check_err_flag(spb_ctx *c) {
-  if (!c->tune[SPB_TUNE_TMA]) return 0;
+  if (c->tune[SPB_TUNE_TMA] == 1) return 0;  // no TMA pass runs
   int h = 0;
   CK(cudaMemcpyAsync(&h, c->err_flag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -1484,14 +1484,15 @@ struct TuneKey {
 };
 std::mutex g_tune_mu;
 struct TuneChoice {
-  int lines, nopdl, g0, split, persist, colw;
+  int lines, nopdl, g0, split, persist, colw, tma;
 };
 std::map<TuneKey, TuneChoice> g_tune_cache;
 
 int apply_choice(spb_ctx *c, const TuneChoice &t) {
   if (spb_ctx_set_tuning(c, SPB_TUNE_ROW_LINES, t.lines) || spb_ctx_set_tuning(c, SPB_TUNE_NO_PDL, t.nopdl) ||
       spb_ctx_set_tuning(c, SPB_TUNE_ROW_G0, t.g0) || spb_ctx_set_tuning(c, SPB_TUNE_SPLIT, t.split) ||
-      spb_ctx_set_tuning(c, SPB_TUNE_PERSIST, t.persist) || spb_ctx_set_tuning(c, SPB_TUNE_COL_WIDTH, t.colw))
+      spb_ctx_set_tuning(c, SPB_TUNE_PERSIST, t.persist) || spb_ctx_set_tuning(c, SPB_TUNE_COL_WIDTH, t.colw) ||
+      spb_ctx_set_tuning(c, SPB_TUNE_TMA, t.tma))
     return -1;
   return 0;
 }
@@ -1523,7 +1524,8 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   const int cur0 = c->cur, xv0 = c->x_valid, xfv0 = c->xf_valid;
   const float xfg0 = c->xf_gamma1;
   const TuneChoice knob0{c->tune[SPB_TUNE_ROW_LINES], c->tune[SPB_TUNE_NO_PDL], c->tune[SPB_TUNE_ROW_G0],
-                         c->tune[SPB_TUNE_SPLIT], c->tune[SPB_TUNE_PERSIST], c->tune[SPB_TUNE_COL_WIDTH]};
+                         c->tune[SPB_TUNE_SPLIT], c->tune[SPB_TUNE_PERSIST], c->tune[SPB_TUNE_COL_WIDTH],
+                         c->tune[SPB_TUNE_TMA]};
   int rc = 0;
   const float2 *bufs[4] = {c->g[0], c->g[1], c->gp, c->X};
   for (int k = 0; k < 4 && !rc; k++)
@@ -1538,7 +1540,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
   const int T = c->nx >= 16 ? c->nx / 16 : 1;
   const int lpb_max = 256 / T > 0 ? 256 / T : 1;
   double best = 1e30;
-  TuneChoice bestc{0, 0, 0, 0, 1, 0};
+  TuneChoice bestc{0, 0, 0, 0, 1, 0, 0};
   // 8-point kernels exist for these row (x) and projection-axis lengths
   auto split_len = [](int n) { return n == 256 || n == 512 || n == 1024 || n == 4096; };
   const int plen = c->nz > 1 ? c->nz : c->ny;
@@ -1573,7 +1575,7 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
     for (int sp = 1; sp <= 2; sp++) {
       if (sp == 2 && (!can_split || li != 0)) continue;
       for (int g0 = 1; g0 <= 2; g0++)
-        for (int nopdl = 0; nopdl <= 1; nopdl++) cands.push_back(TuneChoice{lines, nopdl, g0, sp, 1, 0});
+        for (int nopdl = 0; nopdl <= 1; nopdl++) cands.push_back(TuneChoice{lines, nopdl, g0, sp, 1, 0, 0});
     }
   }
   for (const TuneChoice &t : cands) {
@@ -1581,17 +1583,25 @@ extern "C" int spb_ctx_autotune(spb_ctx *c, const spb_alg_desc *alg, int iterati
     time_choice(t);
   }
   // 2. with the best of those, the projection pass's columns per block
+  //    (plain loads; the built-in width is timed above with its TMA tile
+  //    where that fits, and here with plain loads too)
   if (!rc && bestc.split == 1) {
     const TuneChoice base = bestc;
+    {
+      TuneChoice t = base;
+      t.tma = 1;
+      time_choice(t);
+    }
     for (int w = 1; w <= 16 && !rc; w <<= 1)
       if (col_width_ok(plen, w)) {
         TuneChoice t = base;
         t.colw = w;
+        t.tma = 1;
         time_choice(t);
       }
   }
   // 3. the persistent form, where it applies (no launch-shape knobs)
-  if (!rc && can_persist) time_choice(TuneChoice{0, 0, 1, 1, 2, 0});
+  if (!rc && can_persist) time_choice(TuneChoice{0, 0, 1, 1, 2, 0, 0});
   // restore the state and apply the choice (or the previous knobs on error)
   for (int k = 0; k < 4; k++)
     cudaMemcpyAsync((void *)bufs[k], save + (size_t)k * c->ntot, nc, cudaMemcpyDeviceToDevice, c->st);

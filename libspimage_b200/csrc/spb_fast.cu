@@ -1004,9 +1004,12 @@ static cudaError_t col_fast_launch(const LinePlan &pl, const PassArgs &a, cudaSt
   // shares the line-major amplitude and measured-bit lines of its column
   if (PROJ && a.amp_line && a.meas_bits && (a.meas_words % 4) == 0) {
     if constexpr (PROJ && N >= 64) {
-      // the tile staged by the tensor memory accelerator (knob), built-in width
+      // the tile staged by the tensor memory accelerator at the built-in
+      // width: by default (knob 0) unless another width is asked for, always
+      // with knob 2, never with knob 1
       constexpr int C = col_width<N>();
-      if (a.tma == 2 && tma_fits<N, C>(a)) {
+      const bool want = a.tma == 2 || (a.tma == 0 && (a.col_width == 0 || a.col_width == C));
+      if (want && tma_fits<N, C>(a)) {
         const cudaError_t te = col_tma_launch<N, MODE, C>(pl, a, st);
         if (te != cudaErrorNotSupported) return te;
       }

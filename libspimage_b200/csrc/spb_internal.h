@@ -79,7 +79,8 @@ struct PassArgs {
   int split;
   // columns per block of the projection pass (0: the built-in width); see col_width_ok
   int col_width;
-  // 2: stage the projection pass's column tiles by TMA (spb_fast.cu col_tma_kernel)
+  // projection pass column tiles by TMA (spb_fast.cu col_tma_kernel): 2 always where the
+  // tile fits, 0 where it fits at the built-in width, 1 never
   int tma;
   int *err_flag;  // set by a kernel that could not do its work (device): 1 a bounded wait ran out, 2 a misaligned TMA tile
   // 1: launch the register pass kernels with programmatic dependent launch

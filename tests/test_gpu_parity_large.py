@@ -263,20 +263,22 @@ def test_projection_column_widths_bit_exact(lib, oracle_mod, shape, widths):
         gpu.set_tuning(COL_WIDTH, 3)
 
 
-TMA = 6  # tuning knob: 2 = projection pass column tiles staged by the tensor memory accelerator
+TMA = 6  # tuning knob: 2 = projection pass column tiles staged by the tensor memory accelerator, 1 = plain loads
 
 
+@pytest.mark.parametrize("tma", [2, 1], ids=["tma", "plain"])
 @pytest.mark.parametrize("shape,alg,starts", [((512, 512), HIO, 8), ((1024, 1024), RAAR, None), ((256, 256), DIFFMAP, None),
                                               ((64, 64, 64), HIO, 2), ((128, 128), ER, 3), ((64, 1008), RAAR, None)])
-def test_tma_projection_bit_exact(lib, oracle_mod, shape, alg, starts):
+def test_tma_projection_bit_exact(lib, oracle_mod, shape, alg, starts, tma):
     """The projection pass with its column tiles moved by bulk tensor copies
-    (TMA) gives the oracle's bits: 2-D y lines, 3-D z lines (tile rows of
+    (TMA, the built-in choice where the tile fits) and with plain loads and
+    stores gives the oracle's bits: 2-D y lines, 3-D z lines (tile rows of
     64*64 points), and 64-point columns of 1008-point rows."""
     pat = synth.make_pattern(shape, min(shape) // 4, 1e7, min(shape) / 32.0, seed=9)
     sup = [(AREA, 9, {0: 3.0, 60: 0.7}, 0.05)]
     seeds = list(range(30, 30 + starts)) if starts else None
     gpu = setup_pattern(lib.Phaser(shape), pat, alg, 0.87, sup, seed=30, starts=seeds)
-    gpu.set_tuning(TMA, 2)
+    gpu.set_tuning(TMA, tma)
     gpu.set_tuning(PERSIST, 1)
     assert gpu.iterate(23) == 0
     for k in ([0, starts - 1] if starts else [None]):
