@@ -134,73 +134,139 @@ void sp_srand(int i) { srand((unsigned)i); }
 
 real p_drand48(void) { return (real)(((double)rand()) / (double)RAND_MAX); }
 
-/* n values of p_drand48() into out[], leaving the C library's rand() state
- * exactly where n calls of rand() would leave it.  glibc's rand() is its
- * random() generator: after srand() an additive feedback generator of degree
- * 31 and separation 3 (x[i] = x[i-31] + x[i-3] mod 2^32, output x[i] >> 1).
+/* glibc's rand() is its random() generator: after srand() an additive
+ * feedback generator of degree 31 and separation 3 over 32-bit words,
+ * x[k] = x[k-31] + x[k-3] (mod 2^32), whose output is x[k] >> 1.  Its state
+ * is the last 31 words in a circular array with a front and a rear index;
  * setstate() swaps in another state array and returns the current one, whose
- * leading word then encodes the generator type (mod 5) and the position of
- * its rear pointer (div 5).  When the current state has that form, the values
- * are generated here (no lock and call per value) and the advanced state is
- * handed back with setstate(); otherwise rand() is called n times.
+ * leading word then encodes the generator type (mod 5) and the rear index
+ * (div 5).
  *
- * Two bulk draws never overlap: a process-wide mutex covers the span from
- * the first setstate() to the restoring one, so a second draw cannot take
- * the stand-in state for the real one and leave the generator on it.  If
- * setstate() nevertheless hands back the stand-in (another caller swapped
- * it in), the real state is not ours to restore and the per-value loop is
- * used.  Outside callers of rand()/srand() during a bulk draw act on the
- * stand-in (the drawn values and the final state are the ones above); such
- * concurrent use interleaves unpredictably with a per-value rand() loop
- * too.  The state layout is glibc's: other C libraries take the per-value
- * loop.  No thread of this library calls rand() (the server draws its
- * starts on the device). */
-static void drand_fill(real *out, long long n) {
+ * The recurrence is linear, so the word m steps after a window of 31
+ * consecutive words w[0..30] is a fixed combination of them: with
+ * z^m = c_0 + c_1 z + ... + c_30 z^30 modulo z^31 - z^28 - 1 (coefficients
+ * mod 2^32), x[n+m] = sum_j c_j x[n+j].  A host thread can thus start
+ * anywhere in the sequence: a random-phase start of n pixels is drawn by
+ * several threads, each producing the words of its own span of pixels, and
+ * the C library's state is advanced by n words -- the same values, in the
+ * same pixel order, and the same state as n calls of rand(). */
+enum { RNG_MAX_TYPES = 5, RNG_TYPE_3 = 3, RNG_DEG = 31, RNG_SEP = 3 };
+
+/* a <- a * b mod (z^31 - z^28 - 1), coefficients mod 2^32 */
+static void rng_poly_mulmod(uint32_t *a, const uint32_t *b) {
+  uint32_t prod[2 * RNG_DEG - 1];
+  memset(prod, 0, sizeof(prod));
+  for (int i = 0; i < RNG_DEG; i++)
+    for (int j = 0; j < RNG_DEG; j++) prod[i + j] += a[i] * b[j];
+  /* z^k = z^(k-3) + z^(k-31) for k >= 31, highest terms first */
+  for (int k = 2 * RNG_DEG - 2; k >= RNG_DEG; k--) {
+    prod[k - RNG_SEP] += prod[k];
+    prod[k - RNG_DEG] += prod[k];
+  }
+  memcpy(a, prod, sizeof(uint32_t) * RNG_DEG);
+}
+
+/* c <- c * z mod (z^31 - z^28 - 1) */
+static void rng_poly_mulz(uint32_t *c) {
+  const uint32_t top = c[RNG_DEG - 1];
+  memmove(c + 1, c, sizeof(uint32_t) * (RNG_DEG - 1));
+  c[0] = top;
+  c[RNG_DEG - RNG_SEP] += top;
+}
+
+/* out[j] = x[n+m+j] (j = 0..30) from the window w[j] = x[n+j] */
+static void rng_window_at(const uint32_t *w, long long m, uint32_t *out) {
+  uint32_t c[RNG_DEG], base[RNG_DEG];
+  memset(c, 0, sizeof(c));
+  memset(base, 0, sizeof(base));
+  c[0] = 1;    /* z^0 */
+  base[1] = 1; /* z */
+  for (long long e = m; e > 0; e >>= 1) {
+    if (e & 1) rng_poly_mulmod(c, base);
+    if (e > 1) {
+      uint32_t sq[RNG_DEG];
+      memcpy(sq, base, sizeof(sq));
+      rng_poly_mulmod(base, sq);
+    }
+  }
+  for (int j = 0; j < RNG_DEG; j++) {
+    uint32_t v = 0;
+    for (int i = 0; i < RNG_DEG; i++) v += c[i] * w[i];
+    out[j] = v;
+    rng_poly_mulz(c);
+  }
+}
+
+/* Takes the C library's generator state when it has glibc's TYPE_3 form:
+ * copies the window of its last 31 words into w[] and advances the state by
+ * n words as n calls of rand() would.  Returns 0 (and leaves the state alone)
+ * when the state has another form; the caller then calls rand() itself.
+ *
+ * A process-wide mutex covers the span from the first setstate() to the
+ * restoring one, so two draws cannot take the stand-in state for the real one
+ * and leave the generator on it.  If setstate() nevertheless hands back the
+ * stand-in (another caller swapped it in), the real state is not ours to
+ * advance and 0 is returned.  Outside callers of rand()/srand() during that
+ * short span act on the stand-in; such concurrent use interleaves
+ * unpredictably with a per-value rand() loop too.  No thread of this library
+ * calls rand() (the server draws its starts on the device). */
+static int rng_take(long long n, uint32_t *w) {
 #if defined(__GLIBC__)
-  enum { MAX_TYPES = 5, TYPE_3 = 3, DEG = 31, SEP = 3 };
   static pthread_mutex_t mu = PTHREAD_MUTEX_INITIALIZER;
-  static int32_t holder[DEG + 2]; /* leading word 0: a valid degree-0 state while ours is out */
+  static int32_t holder[RNG_DEG + 2]; /* leading word 0: a valid degree-0 state while ours is out */
+  int ok = 0;
   pthread_mutex_lock(&mu);
   int32_t *cur = (int32_t *)setstate((char *)holder);
   if (cur && cur != holder) {
     const int32_t word = cur[0];
-    if (word >= 0 && word % MAX_TYPES == TYPE_3 && word / MAX_TYPES < DEG) {
+    if (word >= 0 && word % RNG_MAX_TYPES == RNG_TYPE_3 && word / RNG_MAX_TYPES < RNG_DEG) {
       int32_t *x = cur + 1;
-      int r = word / MAX_TYPES, f = (r + SEP) % DEG;
-      for (long long i = 0; i < n; i++) {
-        const uint32_t val = (uint32_t)x[f] + (uint32_t)x[r];
-        x[f] = (int32_t)val;
-        out[i] = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
-        f = f + 1 == DEG ? 0 : f + 1;
-        r = r + 1 == DEG ? 0 : r + 1;
-      }
-      cur[0] = MAX_TYPES * r + TYPE_3;
-      setstate((char *)cur);
-      pthread_mutex_unlock(&mu);
-      return;
+      const int r = word / RNG_MAX_TYPES, f = (r + RNG_SEP) % RNG_DEG;
+      /* slot f holds the oldest word, slot f + j the j-th after it */
+      for (int j = 0; j < RNG_DEG; j++) w[j] = (uint32_t)x[(f + j) % RNG_DEG];
+      /* after n words slot (f + n + j) holds the window at offset n */
+      uint32_t fin[RNG_DEG];
+      rng_window_at(w, n, fin);
+      const int fn = (int)((f + n) % RNG_DEG);
+      for (int j = 0; j < RNG_DEG; j++) x[(fn + j) % RNG_DEG] = (int32_t)fin[j];
+      cur[0] = RNG_MAX_TYPES * (int32_t)((r + n) % RNG_DEG) + RNG_TYPE_3;
+      ok = 1;
     }
     setstate((char *)cur);
   }
   pthread_mutex_unlock(&mu);
+  return ok;
+#else
+  (void)n;
+  (void)w;
+  return 0;
 #endif
-  for (long long i = 0; i < n; i++) out[i] = p_drand48();
 }
 
-/* Random-phase rephasing, split so that the libm work runs on several host
- * threads: the phases are drawn first, in pixel order from the one rand()
- * sequence as the reference draws them; then each pixel's
- * (cos(phase) * |v|, sin(phase) * |v|) is evaluated with the same double
- * libm calls and roundings, on whichever thread -- the same bits. */
+/* Random-phase rephasing of pixels [i0, i1): the words of draws i0.. come
+ * from the window w of the 31 words before draw 0; each pixel's phase is
+ * p_drand48() * 2 pi rounded to float and its value
+ * (cos(phase) * |v|, sin(phase) * |v|) is evaluated with the same double libm
+ * calls and roundings as the reference's loop -- on whichever thread, the
+ * same bits. */
 typedef struct {
   Complex *data;
-  const real *phase;
+  const uint32_t *w;
   long long i0, i1;
 } rephase_span;
 
 static void *rephase_worker(void *arg) {
   const rephase_span *s = (const rephase_span *)arg;
+  uint32_t buf[RNG_DEG];
+  rng_window_at(s->w, s->i0, buf); /* the 31 words before draw i0 */
+  int f = 0, r = RNG_DEG - RNG_SEP;
   for (long long i = s->i0; i < s->i1; i++) {
-    const real phase = s->phase[i];
+    const uint32_t val = buf[f] + buf[r];
+    buf[f] = val;
+    f = f + 1 == RNG_DEG ? 0 : f + 1;
+    r = r + 1 == RNG_DEG ? 0 : r + 1;
+    const real u = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
+    const real phase = u * 3.14159265358979323846 * 2;
     const real amp = sp_cabs(s->data[i]);
     s->data[i].re = cos(phase) * amp;
     s->data[i].im = sin(phase) * amp;
@@ -209,7 +275,7 @@ static void *rephase_worker(void *arg) {
 }
 
 #define REPHASE_MAX_THREADS 32
-static void rephase_parallel(Complex *data, const real *phase, long long n) {
+static void rephase_parallel(Complex *data, const uint32_t *w, long long n) {
   long long nt = n >= (1 << 16) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
   if (nt < 1) nt = 1;
   if (nt > REPHASE_MAX_THREADS) nt = REPHASE_MAX_THREADS;
@@ -218,7 +284,7 @@ static void rephase_parallel(Complex *data, const real *phase, long long n) {
   int started[REPHASE_MAX_THREADS] = {0};
   for (long long t = 0; t < nt; t++) {
     span[t].data = data;
-    span[t].phase = phase;
+    span[t].w = w;
     span[t].i0 = n * t / nt;
     span[t].i1 = n * (t + 1) / nt;
     if (t > 0) started[t] = pthread_create(&th[t], NULL, rephase_worker, &span[t]) == 0;
@@ -236,20 +302,18 @@ void sp_image_rephase(Image *img, int type) {
   if (type == SP_ZERO_PHASE) {
     for (long long i = 0; i < n; i++) img->image->data[i] = sp_cinit(sp_cabs(img->image->data[i]), 0);
   } else if (type == SP_RANDOM_PHASE) {
-    real *phase = (real *)malloc(sizeof(real) * (size_t)(n > 0 ? n : 1));
-    if (!phase) { /* no scratch: one pass, as the reference */
-      for (long long i = 0; i < n; i++) {
-        const real ph = p_drand48() * 3.14159265358979323846 * 2;
-        const real amp = sp_cabs(img->image->data[i]);
-        img->image->data[i].re = cos(ph) * amp;
-        img->image->data[i].im = sin(ph) * amp;
-      }
+    uint32_t w[RNG_DEG];
+    if (n > 0 && rng_take(n, w)) {
+      rephase_parallel(img->image->data, w, n);
       return;
     }
-    drand_fill(phase, n);
-    for (long long i = 0; i < n; i++) phase[i] = phase[i] * 3.14159265358979323846 * 2;
-    rephase_parallel(img->image->data, phase, n);
-    free(phase);
+    /* another generator layout: one rand() per pixel, as the reference */
+    for (long long i = 0; i < n; i++) {
+      const real ph = p_drand48() * 3.14159265358979323846 * 2;
+      const real amp = sp_cabs(img->image->data[i]);
+      img->image->data[i].re = cos(ph) * amp;
+      img->image->data[i].im = sin(ph) * amp;
+    }
   }
 }
 

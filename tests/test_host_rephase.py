@@ -2,8 +2,11 @@
 src/image_util.c:1035-1067): the values come from the C library's rand()
 sequence and libm's double cos/sin exactly as the reference computes them
 one pixel at a time, although this library draws the sequence in bulk from
-the generator's state and evaluates cos/sin on several threads; and rand()
-continues afterwards as if it had been called once per pixel."""
+the generator's state -- each host thread jumping ahead to its own span of
+pixels -- and evaluates cos/sin on those threads; and rand() continues
+afterwards as if it had been called once per pixel.  Sizes cover draws
+shorter than the generator's 31-word state, one thread, and uneven spans
+over all host threads."""
 import ctypes as C
 
 import numpy as np
@@ -41,7 +44,8 @@ def _expected(libc, libm, amp, seed, skip):
     return out, libc.rand()
 
 
-@pytest.mark.parametrize("shape,seed,skip", [((16, 16), 3, 0), ((300, 300), 11, 5), ((1, 70001), 0, 31)])
+@pytest.mark.parametrize("shape,seed,skip", [((16, 16), 3, 0), ((300, 300), 11, 5), ((1, 70001), 0, 31),
+                                             ((1, 7), 2, 1), ((1, 30), 4, 40), ((257, 263), 9, 2)])
 def test_rephase_matches_per_pixel_draws(env, shape, seed, skip):
     L, so, libc, libm = env
     amp = (np.random.default_rng(seed).random(shape) * 4).astype(np.float32)
