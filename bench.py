@@ -61,7 +61,27 @@ WORKLOADS = {
         blur={0: 3.0, 1000: 0.7}, constraints=2,
         desc="plain HIO 256x256 FP32: 1000 HIO (beta 0.9, area support every 20, area 0.05, blur 3.0->0.7)",
     ),
+    "hio1000": dict(
+        pattern="hio1000", shape=(1000, 1000), stages=[("HIO", 0.9, 1000)], period=20, area=0.05,
+        blur={0: 3.0, 1000: 0.7}, constraints=2,
+        desc="plain HIO 1000x1000 FP32 (a job size of the mixed batch: 250 blob, 1e7 photons, beamstop 11.8 px): "
+             "1000 HIO (beta 0.9, area support every 20, area 0.05, blur 3.0->0.7)",
+    ),
 }
+
+# launch-shape knobs of spb_ctx_set_tuning by name (--tune; they change no
+# arithmetic): for timing and profiling the other kernel forms
+TUNE_KNOBS = {"row_lines": 0, "no_pdl": 1, "row_g0": 2, "split": 3, "persist": 4, "col_width": 5, "tma": 6}
+
+
+def parse_tune(items):
+    out = {}
+    for it in items or []:
+        k, _, v = it.partition("=")
+        if k not in TUNE_KNOBS or not v.lstrip("-").isdigit():
+            raise SystemExit(f"--tune {it}: expected one of {sorted(TUNE_KNOBS)}=<int>")
+        out[k] = int(v)
+    return out
 
 # algorithmic HBM bytes per pixel of the dominant 2-D kernels (bit-packed
 # support/measured masks): row pass reads Y + g_prev, writes g_new + X
@@ -195,6 +215,9 @@ def gpu_arm(args):
     amp, mask, support, _ = synth.workload(wl["pattern"], seed=0)
     L.load()
     ph, handles = build_phaser(L, wl, amp, mask, support, seed=rank)
+    tune = parse_tune(args.tune)
+    for k, v in tune.items():
+        ph.set_tuning(TUNE_KNOBS[k], v)
     stream = torch.cuda.Stream()
     ph.set_stream(stream.cuda_stream)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
@@ -297,7 +320,7 @@ def gpu_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wl["desc"], "shape": list(wl["shape"]), "slots_per_step": slots,
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before each timed step",
-                       "efourier_final_e2e": efour, "error_vs_fp64": fp64},
+                       "efourier_final_e2e": efour, "error_vs_fp64": fp64, **({"tuning": tune} if tune else {})},
             "e2e": {"value": round(e2e_val, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches_total),
             "kernels": {k: {"launches": v[0], "avg_us": round(v[1] / max(v[0], 1) * 1e3, 3)} for k, v in ktimes.items()},
@@ -848,6 +871,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="raar1024", choices=sorted(k for k in WORKLOADS if "starts" not in WORKLOADS[k]))
+    ap.add_argument("--tune", action="append", default=[], metavar="KNOB=VALUE",
+                    help=f"launch-shape knob of the headline phaser (repeatable): {', '.join(sorted(TUNE_KNOBS))}")
     ap.add_argument("--cpu-sample-slots", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=2, help="timed whole jobs of the batched block (0: skip it)")

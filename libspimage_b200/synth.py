@@ -24,6 +24,7 @@ WORKLOADS = {
     "raar1024": ((1024, 1024), 256, 1e8, 8),
     "batch512": ((512, 512), 128, 1e7, 6),
     "vol128": ((128, 128, 128), 32, 1e8, 3),
+    "hio1000": ((1000, 1000), 250, 1e7, 1000 / 85.0),
 }
 
 
