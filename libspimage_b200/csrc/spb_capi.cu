@@ -1298,7 +1298,7 @@ static int select_and_mask(spb_ctx *c, const float *absv, long long n, int nb, i
                            uint8_t *flags, const SupportParams *dev = nullptr) {
   if (prof_begin(c)) return -1;
   if (select_and_mask_on(c->st, c->sel, absv, n, nb, type, value, flags, dev)) return -1;
-  c->launches += (type == SPB_SUPPORT_AREA) ? 10 : 4;
+  c->launches += (type == SPB_SUPPORT_AREA) ? 6 : 4;  // init, four histogram passes, mask | init, max, finish, mask
   return prof_end(c, type == SPB_SUPPORT_AREA ? 16 : 17);
 }
 

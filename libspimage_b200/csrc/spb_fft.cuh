@@ -277,7 +277,9 @@ __host__ __device__ constexpr int ct_max_butterflies(int n) {
 
 // The stages of stage_fixed with the plan, the strides and the divisions known
 // at compile time; twiddles from the per-stage table ([stage][m-1][k], the
-// same float values as tw[m*k*tstep]), so the arithmetic is unchanged.
+// same float values as tw[m*k*tstep]; N - 1 entries in all), read from
+// shared memory where the kernel staged it, else from global memory, so the
+// arithmetic is unchanged.
 template <int N, int S, int NS, bool INV>
 struct CtStages {
   static __device__ float2 *run(float2 *x, float2 *y, const float2 *__restrict__ stw, int es, int t0, int tn) {
@@ -291,7 +293,7 @@ struct CtStages {
       if (NS > 1 && k) {
 #pragma unroll
         for (int m = 1; m < R; m++) {
-          float2 w = __ldg(stw + (m - 1) * NS + k);
+          float2 w = stw[(m - 1) * NS + k];  // shared-memory or global table
           if (INV) w.y = -w.y;
           a[m] = cmulw(a[m], w.x, w.y);
         }
@@ -337,10 +339,12 @@ __device__ float2 *line_fft(float2 *bufA, float2 *bufB, const LinePlan &p, int e
 }  // namespace spb
 
 namespace spb {
-// line_fft with the plan fixed at compile time when NC > 0
+// line_fft with the plan fixed at compile time when NC > 0 (stage table `stw`:
+// p.stw or a shared-memory copy of it)
 template <bool INV, int NC>
-__device__ __forceinline__ float2 *line_fft_sel(float2 *bufA, float2 *bufB, const LinePlan &p, int es, int t0, int tn) {
-  if constexpr (NC > 0) return CtStages<NC, 0, 1, INV>::run(bufA, bufB, p.stw, es, t0, tn);
+__device__ __forceinline__ float2 *line_fft_sel(float2 *bufA, float2 *bufB, const LinePlan &p, int es, int t0, int tn,
+                                               const float2 *stw) {
+  if constexpr (NC > 0) return CtStages<NC, 0, 1, INV>::run(bufA, bufB, stw, es, t0, tn);
   else return line_fft<INV>(bufA, bufB, p, es, t0, tn);
 }
 }  // namespace spb

@@ -106,14 +106,20 @@ struct PassArgs {
   float n_f;        // (float)N
 };
 
+// Radix select state of one start: pass p (0..3) histograms the 8-bit digit
+// of the keys that match pass_prefix[p] under pass_mask[p] into hist[p]; the
+// digit picked from it narrows the prefix for pass p + 1 (pass_rank[p] is the
+// rank sought among the keys matching pass p's prefix, 0-based, descending).
 struct SelectState {
-  unsigned int prefix;       // key bits fixed so far
-  unsigned int prefix_mask;  // which bits are fixed
-  unsigned long long rank;   // remaining rank (0-based) within the prefix bucket, descending
-  unsigned int hist[2048];
-  float result;
+  unsigned long long rank;  // rank sought among all keys (pass 0)
+  unsigned int hist[4][256];
+  unsigned int pass_prefix[4], pass_mask[4];
+  unsigned long long pass_rank[4];
+  unsigned int reserved[1010];
+  float result;  // the selected key (area rule) or the maximum (threshold rule)
   unsigned int maxbits;
 };
+static_assert(sizeof(SelectState) == 8216, "the selection state keeps its size");
 
 // register-resident kernels (spb_fast.cu); cudaErrorNotSupported when the
 // line length or mode has none
@@ -143,7 +149,7 @@ cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArg
 cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long long k, SelectState *state,
                                    cudaStream_t st, const unsigned long long *k_dev = nullptr);
 cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st);
-cudaError_t launch_mask_from_abs(const float *absv, const SelectState *state, float rel, int use_rel, uint8_t *flags,
+cudaError_t launch_mask_from_abs(const float *absv, SelectState *state, float rel, int use_rel, uint8_t *flags,
                                  long long n, int nb, cudaStream_t st, const float *rel_dev = nullptr);
 // out[b*4 + k]; scratch of reduce_scratch_doubles(nb) doubles starting at out
 int reduce_scratch_doubles(int nb);

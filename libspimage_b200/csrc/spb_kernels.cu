@@ -18,7 +18,8 @@ namespace spb {
 
 // ---------------------------------------------------------------- row pass
 template <int MODE, int NC>
-__global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, int tpr, int rpb, long long nrows) {
+__device__ __forceinline__ void row_pass_body(const LinePlan &px, const PassArgs &a, int tpr, int rpb,
+                                              long long nrows) {
   extern __shared__ float2 smem[];
   const int n = px.n;
   const int lr = threadIdx.x / tpr, t = threadIdx.x % tpr;
@@ -68,11 +69,11 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
 
   if constexpr (MODE == ROW_FWD || MODE == ROW_FWD_DEPHASE || MODE == ROW_FWD_F32 || MODE == ROW_FWD_SQUARE_F32 ||
                 MODE == ROW_DM_F1_FWD) {
-    float2 *r = line_fft_sel<false, NC>(A, B, px, 1, t, tpr);
+    float2 *r = line_fft_sel<false, NC>(A, B, px, 1, t, tpr, px.stw);
     if (valid)
       for (int i = t; i < n; i += tpr) a.dst[base + i] = r[i];
   } else if constexpr (MODE == ROW_INV || MODE == ROW_INV_SCALE || MODE == ROW_INV_ABS) {
-    float2 *r = line_fft_sel<true, NC>(A, B, px, 1, t, tpr);
+    float2 *r = line_fft_sel<true, NC>(A, B, px, 1, t, tpr, px.stw);
     if (valid) {
       for (int i = t; i < n; i += tpr) {
         if constexpr (MODE == ROW_INV) a.dst[base + i] = r[i];
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
   } else if constexpr (MODE == ROW_ITER) {
     const float beta = iter_beta(a);
     const float one_m2b = fsub(1.0f, fmul(2.0f, beta));  // 1 - 2*beta in float, as the reference
-    float2 *r = line_fft_sel<true, NC>(A, B, px, 1, t, tpr);
+    float2 *r = line_fft_sel<true, NC>(A, B, px, 1, t, tpr, px.stw);
     for (int i = t; i < n; i += tpr) {
       float2 g = make_float2(0.0f, 0.0f);
       if (valid) {
@@ -108,13 +109,13 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
     }
     __syncthreads();
     float2 *o = (r == A) ? B : A;
-    float2 *x = line_fft_sel<false, NC>(r, o, px, 1, t, tpr);
+    float2 *x = line_fft_sel<false, NC>(r, o, px, 1, t, tpr, px.stw);
     if (valid)
       for (int i = t; i < n; i += tpr) a.dst[base + i] = x[i];
   } else if constexpr (MODE == ROW_DM_ITER) {
     const float beta = iter_beta(a);
-    float2 *rho = line_fft_sel<true, NC>(A, B, px, 1, t, tpr);
-    float2 *fr = line_fft_sel<true, NC>(Cb, D, px, 1, t, tpr);
+    float2 *rho = line_fft_sel<true, NC>(A, B, px, 1, t, tpr, px.stw);
+    float2 *fr = line_fft_sel<true, NC>(Cb, D, px, 1, t, tpr, px.stw);
     for (int i = t; i < n; i += tpr) {
       float2 g = make_float2(0.0f, 0.0f), f1 = g;
       if (valid) {
@@ -139,9 +140,9 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
     }
     __syncthreads();
     float2 *o1 = (rho == A) ? B : A;
-    float2 *x = line_fft_sel<false, NC>(rho, o1, px, 1, t, tpr);
+    float2 *x = line_fft_sel<false, NC>(rho, o1, px, 1, t, tpr, px.stw);
     float2 *o2 = (fr == Cb) ? D : Cb;
-    float2 *xf = line_fft_sel<false, NC>(fr, o2, px, 1, t, tpr);
+    float2 *xf = line_fft_sel<false, NC>(fr, o2, px, 1, t, tpr, px.stw);
     if (valid)
       for (int i = t; i < n; i += tpr) {
         a.dst[base + i] = x[i];
@@ -150,9 +151,32 @@ __global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, 
   }
 }
 
-// ------------------------------------------------------------- column pass
 template <int MODE, int NC>
-__global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a, int ct, int tpc) {
+__global__ void __launch_bounds__(256) row_pass_kernel(LinePlan px, PassArgs a, int tpr, int rpb, long long nrows) {
+  row_pass_body<MODE, NC>(px, a, tpr, rpb, nrows);
+}
+
+// 1000-point rows (the mixed batches' largest non-power-of-two length) run
+// as one row of 200 threads per block with at most 32 registers, so that nine
+// blocks share an SM and a 1000-row pattern takes one wave (the difference
+// map's iteration keeps the general kernel).  Measured on one B200, HIO
+// 1000x1000 per slot: 43.2 us with the general budget (42 registers), 43.6
+// with 40, 39.9 with 32 (a few bytes of spills, more blocks in flight).
+template <int MODE>
+__global__ void __maxnreg__(32)
+    row_pass_kernel_1000(LinePlan px, PassArgs a, int tpr, int rpb, long long nrows) {
+  row_pass_body<MODE, 1000>(px, a, tpr, rpb, nrows);
+}
+
+// ------------------------------------------------------------- column pass
+// byte offset of the stage table behind a column block's buffers (16-byte aligned)
+__host__ __device__ constexpr size_t col_tw_offset(int n, int ct, bool proj) {
+  return ((size_t)2 * n * ct * 8 + (proj ? (size_t)n * ct * 5 : 0) + 15) / 16 * 16;
+}
+
+// compile-time plans read their stage table from shared memory
+template <int MODE, int NC>
+__device__ __forceinline__ void col_pass_body(const LinePlan &pl, const PassArgs &a, int ct, int tpc) {
   extern __shared__ float2 smem[];
   const int n = pl.n;
   const int cc = threadIdx.x % ct, t = threadIdx.x / ct;
@@ -168,6 +192,9 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
   float *AMc = reinterpret_cast<float *>(smem + (size_t)2 * n * ct) + cc;
   uint8_t *FLc = reinterpret_cast<uint8_t *>(reinterpret_cast<float *>(smem + (size_t)2 * n * ct) + (size_t)n * ct) + cc;
   const long long ai0 = PROJ ? lbase % a.n_start : 0;
+  float2 *TW = reinterpret_cast<float2 *>(reinterpret_cast<unsigned char *>(smem) + col_tw_offset(n, ct, PROJ));
+  if constexpr (NC > 0)
+    for (int i = threadIdx.x; i < NC - 1; i += blockDim.x) TW[i] = pl.stw[i];
 
   for (int i = t; i < n; i += tpc) {
     float2 v = make_float2(0.0f, 0.0f);
@@ -189,11 +216,11 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
 
   float2 *r;
   if constexpr (MODE == COL_FWD) {
-    r = line_fft_sel<false, NC>(A, B, pl, ct, t, tpc);
+    r = line_fft_sel<false, NC>(A, B, pl, ct, t, tpc, TW);
   } else if constexpr (MODE == COL_INV || MODE == COL_INV_SQUARE_F32) {
-    r = line_fft_sel<true, NC>(A, B, pl, ct, t, tpc);
+    r = line_fft_sel<true, NC>(A, B, pl, ct, t, tpc, TW);
   } else {
-    float2 *f = line_fft_sel<false, NC>(A, B, pl, ct, t, tpc);
+    float2 *f = line_fft_sel<false, NC>(A, B, pl, ct, t, tpc, TW);
     if (valid) {
       for (int i = t; i < n; i += tpc) {
         const long long idx = lbase + i * a.estride;
@@ -206,10 +233,23 @@ __global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a,
     }
     __syncthreads();
     float2 *o2 = (f == A) ? B : A;
-    r = line_fft_sel<true, NC>(f, o2, pl, ct, t, tpc);
+    r = line_fft_sel<true, NC>(f, o2, pl, ct, t, tpc, TW);
   }
   if (valid)
     for (int i = t; i < n; i += tpc) a.dst[lbase + i * a.estride] = r[(size_t)i * ct];
+}
+
+template <int MODE, int NC>
+__global__ void __launch_bounds__(1024) col_pass_kernel(LinePlan pl, PassArgs a, int ct, int tpc) {
+  col_pass_body<MODE, NC>(pl, a, ct, tpc);
+}
+
+// 1000-point columns run as four columns of 200 threads per block with at
+// most 32 registers, so that two blocks share an SM (a 1000-column pattern:
+// 250 blocks, one wave)
+template <int MODE>
+__global__ void __maxnreg__(32) col_pass_kernel_1000(LinePlan pl, PassArgs a, int ct, int tpc) {
+  col_pass_body<MODE, 1000>(pl, a, ct, tpc);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -254,6 +294,7 @@ static cudaError_t row_launch_n(const LinePlan &px, const PassArgs &a, cudaStrea
   // transform buffers, then (UPD) a slab of g0 and rpb*n bytes of flags
   const size_t smem = (size_t)(nbuf + (UPD ? 1 : 0)) * rpb * n * sizeof(float2) + (UPD ? (size_t)rpb * n : 0);
   auto k = row_pass_kernel<MODE, NC>;
+  if constexpr (NC == 1000 && MODE != ROW_DM_ITER) k = row_pass_kernel_1000<MODE>;
   static size_t done = 0;
   cudaError_t e = smem_attr(k, smem, done);
   if (e != cudaSuccess) return e;
@@ -331,9 +372,12 @@ static cudaError_t col_launch_n(const LinePlan &pl, const PassArgs &a, cudaStrea
   if (tpc * ct > 1024) tpc = 1024 / ct;
   if (tpc * ct < 32) tpc = 32 / ct;
   constexpr bool PROJ = (MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC);
-  // two transform buffers, then (projection) n*ct amplitudes and n*ct flag bytes
-  const size_t smem = (size_t)2 * n * ct * sizeof(float2) + (PROJ ? (size_t)n * ct * (sizeof(float) + 1) : 0);
+  // two transform buffers, then (projection) n*ct amplitudes and n*ct flag
+  // bytes, then (compile-time plans) the n - 1 entries of the stage table
+  const size_t smem = NC > 0 ? col_tw_offset(n, ct, PROJ) + (size_t)(NC - 1) * sizeof(float2)
+                             : (size_t)2 * n * ct * sizeof(float2) + (PROJ ? (size_t)n * ct * (sizeof(float) + 1) : 0);
   auto k = col_pass_kernel<MODE, NC>;
+  if constexpr (NC == 1000) k = col_pass_kernel_1000<MODE>;
   static size_t done = 0;
   cudaError_t e = smem_attr(k, smem, done);
   if (e != cudaSuccess) return e;
@@ -405,22 +449,82 @@ cudaError_t launch_gauss_table(const PassArgs &a, float *tab, cudaStream_t st) {
 // holding the same digit are combined with a match before the atomic,
 // because the leading digits of |blur| concentrate in a few bins.  Start b
 // owns v[b*n .. (b+1)*n) and state s[b]; the grid's y dimension runs over
-// starts.
+// starts.  The digit a pass picks is found at the start of the next pass
+// (and of the mask kernel, after the last) by warp 0 of every block from the
+// previous pass's histogram, so the selection takes one launch per pass.
 #define SEL_BITS 8
 #define SEL_BINS 256
 // Each thread loads SEL_UNROLL keys (independent loads in flight) before it
 // bins them; a warp skips the match when none of its keys carries the prefix.
 #define SEL_UNROLL 8
+
+// Warp 0 of a block: the digit of histogram `hist` (digits at `shift` of the
+// keys matching prefix/mask) that holds the rank-th largest of those keys,
+// and the narrowed prefix, mask and rank.  Lane l owns digits [8l, 8l+8);
+// the keys with a larger digit are counted from the higher lanes.  Results in
+// out[0..1] (prefix, mask) and *orank, shared by the block.
+__device__ void select_pick_warp(const unsigned int *hist, unsigned long long rank, unsigned int prefix,
+                                 unsigned int mask, int shift, unsigned int *out, unsigned long long *orank) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long own = 0;
+  unsigned int c[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    c[j] = hist[lane * 8 + j];
+    own += c[j];
+  }
+  unsigned long long above = 0;
+  for (int l = 31; l > 0; l--) {
+    const unsigned long long x = __shfl_sync(0xffffffffu, own, l);
+    if (l > lane) above += x;
+  }
+  if (lane == 0) {  // unchanged unless a lane finds the digit (it always does: rank < the count)
+    out[0] = prefix;
+    out[1] = mask;
+    *orank = rank;
+  }
+  __syncwarp();
+  unsigned long long cum = above;
+#pragma unroll
+  for (int j = 7; j >= 0; j--) {
+    if (cum <= rank && cum + c[j] > rank) {
+      out[0] = prefix | ((unsigned int)(lane * 8 + j) << shift);
+      out[1] = mask | ((unsigned int)(SEL_BINS - 1) << shift);
+      *orank = rank - cum;
+    }
+    cum += c[j];
+  }
+}
+
 __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restrict__ v, long long n, SelectState *s,
-                                                          int shift) {
+                                                          int pass) {
   __shared__ unsigned int h[8][SEL_BINS];
+  __shared__ unsigned int pm[2];
+  __shared__ unsigned long long pr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int b = blockIdx.y;
   v += (long long)b * n;
   s += b;
   for (int i = threadIdx.x; i < 8 * SEL_BINS; i += blockDim.x) (&h[0][0])[i] = 0;
+  if (pass == 0) {
+    if (threadIdx.x == 0) {
+      pm[0] = s->pass_prefix[0];
+      pm[1] = s->pass_mask[0];
+    }
+  } else if (warp == 0) {
+    // the digit the previous pass picks: narrows the prefix for this pass
+    const int q = pass - 1;
+    select_pick_warp(s->hist[q], s->pass_rank[q], s->pass_prefix[q], s->pass_mask[q], 24 - SEL_BITS * q, pm, &pr);
+    __syncwarp();
+    if (lane == 0 && blockIdx.x == 0) {
+      s->pass_prefix[pass] = pm[0];
+      s->pass_mask[pass] = pm[1];
+      s->pass_rank[pass] = pr;
+    }
+  }
   __syncthreads();
-  const unsigned int prefix = s->prefix, pmask = s->prefix_mask;
+  const int shift = 24 - SEL_BITS * pass;
+  const unsigned int prefix = pm[0], pmask = pm[1];
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long start = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long rounds = (n + stride * SEL_UNROLL - 1) / (stride * SEL_UNROLL);
@@ -445,55 +549,18 @@ __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restric
   for (int d = threadIdx.x; d < SEL_BINS; d += blockDim.x) {
     unsigned int c = 0;
     for (int w = 0; w < 8; w++) c += h[w][d];
-    if (c) atomicAdd(&s->hist[d], c);
+    if (c) atomicAdd(&s->hist[pass][d], c);
   }
-}
-
-// one warp per start: find the digit holding the rank-th largest key, narrow the prefix
-__global__ void select_pick_kernel(SelectState *states, int shift, int last) {
-  SelectState *s = states + blockIdx.x;
-  const int lane = threadIdx.x;
-  // lane l owns digits [8l, 8l+8); counts of keys with a larger digit come from the higher lanes
-  unsigned long long own = 0;
-  unsigned int c[8];
-  for (int j = 0; j < 8; j++) {
-    c[j] = s->hist[lane * 8 + j];
-    own += c[j];
-  }
-  unsigned long long above = 0;
-  for (int l = 31; l > 0; l--) {
-    const unsigned long long x = __shfl_sync(0xffffffffu, own, l);
-    if (l > lane) above += x;
-  }
-  const unsigned long long rank = s->rank;
-  unsigned long long cum = above;
-  int pick = -1;
-  unsigned long long newrank = 0;
-  for (int j = 7; j >= 0; j--) {
-    if (pick < 0 && cum + c[j] > rank && cum <= rank) {
-      pick = lane * 8 + j;
-      newrank = rank - cum;
-    }
-    cum += c[j];
-  }
-  __syncwarp();
-  if (pick >= 0) {
-    s->prefix |= ((unsigned int)pick) << shift;
-    s->prefix_mask |= ((unsigned int)(SEL_BINS - 1)) << shift;
-    s->rank = newrank;
-    if (last) s->result = __uint_as_float(s->prefix);
-  }
-  __syncwarp();
-  for (int j = 0; j < 8; j++) s->hist[lane * 8 + j] = 0;
 }
 
 __global__ void select_init_kernel(SelectState *states, unsigned long long rank, const unsigned long long *rank_dev) {
   SelectState *s = states + blockIdx.x;
-  for (int d = threadIdx.x; d < 2048; d += blockDim.x) s->hist[d] = 0;
+  for (int d = threadIdx.x; d < 4 * SEL_BINS; d += blockDim.x) (&s->hist[0][0])[d] = 0;
   if (threadIdx.x == 0) {
-    s->prefix = 0;
-    s->prefix_mask = 0;
     s->rank = rank_dev ? *rank_dev : rank;
+    s->pass_prefix[0] = 0;
+    s->pass_mask[0] = 0;
+    s->pass_rank[0] = s->rank;
     s->maxbits = 0;
   }
 }
@@ -506,15 +573,12 @@ static unsigned blocks_per_start(long long n, int nb) {
   return (unsigned)(b > 0 ? b : 1);
 }
 
+// the four histogram passes; the last pick happens in the mask kernel
 cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long long k, SelectState *state,
                                    cudaStream_t st, const unsigned long long *k_dev) {
   select_init_kernel<<<nb, 256, 0, st>>>(state, (unsigned long long)k, k_dev);
   const dim3 grid(blocks_per_start(n, nb), nb);
-  for (int p = 0; p < 4; p++) {
-    const int shift = 24 - SEL_BITS * p;
-    select_hist_kernel<<<grid, 256, 0, st>>>(absv, n, state, shift);
-    select_pick_kernel<<<nb, 32, 0, st>>>(state, shift, p == 3);
-  }
+  for (int p = 0; p < 4; p++) select_hist_kernel<<<grid, 256, 0, st>>>(absv, n, state, p);
   return cudaGetLastError();
 }
 
@@ -542,12 +606,27 @@ cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *
   return cudaGetLastError();
 }
 
-// support_from_absolute_threshold (src/support_update.c:392-400): strict '>'
-__global__ void mask_kernel(const float *__restrict__ v, const SelectState *states, float rel, int use_rel,
+// support_from_absolute_threshold (src/support_update.c:392-400): strict '>'.
+// Threshold: the maximum times rel (use_rel), or the key the radix select's
+// last pass picks (found here by warp 0 of every block; block 0 records it).
+__global__ void mask_kernel(const float *__restrict__ v, SelectState *states, float rel, int use_rel,
                             uint8_t *flags, long long n, const float *rel_dev) {
+  __shared__ unsigned int pm[2];
+  __shared__ unsigned long long pr;
   const int b = blockIdx.y;
-  const SelectState *s = states + b;
-  const float t = use_rel ? __fmul_rn(s->result, rel_dev ? *rel_dev : rel) : s->result;
+  SelectState *s = states + b;
+  float t;
+  if (use_rel) {
+    t = __fmul_rn(s->result, rel_dev ? *rel_dev : rel);
+  } else {
+    if (threadIdx.x < 32) {
+      select_pick_warp(s->hist[3], s->pass_rank[3], s->pass_prefix[3], s->pass_mask[3], 0, pm, &pr);
+      __syncwarp();
+      if (threadIdx.x == 0 && blockIdx.x == 0) s->result = __uint_as_float(pm[0]);
+    }
+    __syncthreads();
+    t = __uint_as_float(pm[0]);
+  }
   v += (long long)b * n;
   flags += (long long)b * n;
   // four elements per thread and round, their loads in flight together
@@ -569,7 +648,7 @@ __global__ void mask_kernel(const float *__restrict__ v, const SelectState *stat
   }
 }
 
-cudaError_t launch_mask_from_abs(const float *absv, const SelectState *state, float rel, int use_rel, uint8_t *flags,
+cudaError_t launch_mask_from_abs(const float *absv, SelectState *state, float rel, int use_rel, uint8_t *flags,
                                  long long n, int nb, cudaStream_t st, const float *rel_dev) {
   mask_kernel<<<dim3(blocks_per_start(n, nb), nb), 256, 0, st>>>(absv, state, rel, use_rel, flags, n, rel_dev);
   return cudaGetLastError();
