@@ -67,6 +67,12 @@ WORKLOADS = {
         desc="plain HIO 1000x1000 FP32 (a job size of the mixed batch: 250 blob, 1e7 photons, beamstop 11.8 px): "
              "1000 HIO (beta 0.9, area support every 20, area 0.05, blur 3.0->0.7)",
     ),
+    "vol128": dict(
+        pattern="vol128", shape=(128, 128, 128), stages=[("HIO", 0.9, 1000)], period=20, area=0.05,
+        blur={0: 3.0, 1000: 0.7}, constraints=2,
+        desc="plain HIO 128^3 FP32 (the volume of the mixed batch and the serving mix: 32^3 blob, 1e8 photons, "
+             "spherical beamstop 3 px): 1000 HIO (beta 0.9, area support every 20, area 0.05, blur 3.0->0.7)",
+    ),
 }
 
 # launch-shape knobs of spb_ctx_set_tuning by name (--tune; they change no

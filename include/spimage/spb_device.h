@@ -97,8 +97,12 @@ const char *spb_kernel_name(int kind);
  * column tiles -- 0 (the built-in choice) with the tensor memory accelerator
  * (bulk tensor loads under an mbarrier and bulk tensor stores) where the
  * tile fits and no other column width is asked for, 2 with it wherever the
- * tile fits, 1 with plain loads and stores.  Setting a knob drops the
- * context's captured graphs. */
+ * tile fits, 1 with plain loads and stores; SPB_TUNE_PLANE: how a 3-D
+ * volume with ny = nz = 64 or 128 runs the y and z parts of an iteration --
+ * 2 as one plane pass (one block per x-plane: forward y, forward z,
+ * projection, inverse z, inverse y; measured slower than the column passes
+ * on the B200), 0 (the built-in choice) or 1 as three column passes.
+ * Setting a knob drops the context's captured graphs. */
 enum {
   SPB_TUNE_ROW_LINES = 0,
   SPB_TUNE_NO_PDL = 1,
@@ -107,7 +111,8 @@ enum {
   SPB_TUNE_PERSIST = 4,
   SPB_TUNE_COL_WIDTH = 5,
   SPB_TUNE_TMA = 6,
-  SPB_TUNE_KNOBS = 7
+  SPB_TUNE_PLANE = 7,
+  SPB_TUNE_KNOBS = 8
 };
 int spb_ctx_set_tuning(spb_ctx *ctx, int knob, int value);
 int spb_ctx_get_tuning(spb_ctx *ctx, int knob);

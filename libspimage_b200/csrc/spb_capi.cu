@@ -368,12 +368,39 @@ int other_axes(const spb_ctx *c, int *axes) {
   return k;
 }
 
+// The projection of a 3-D volume with ny = nz = 64 or 128 as one plane pass
+// (spb_fast.cu plane_kernel) instead of three column passes, when
+// SPB_TUNE_PLANE is 2.  Not the built-in choice: measured on one B200, HIO
+// 128^3 per slot, three column passes / plane pass: 38.9 / 63.6 us for one
+// start, 266 / 441 us for 8 starts -- a 140 KB plane per block leaves one
+// block of 32 warps per SM for four transforms, while the column passes
+// spread the same transforms over many small blocks.  Returns 1 when it ran,
+// 0 when it does not apply (the column passes run), -1 on error.
+static int plane_pass(spb_ctx *c, int mode, const float2 *src, float2 *dst, PassArgs a) {
+  if (c->tune[SPB_TUNE_PLANE] != 2 || !plane_fits(mode, c->az.lp, a)) return 0;
+  a.src = src;
+  a.dst = dst;
+  a.line_axis = 2;
+  if (prof_begin(c)) return -1;
+  for (int o0 = 0; o0 < c->nb; o0 += kMaxGridY) {
+    a.outer0 = o0;
+    a.nouter = c->nb - o0 < kMaxGridY ? c->nb - o0 : kMaxGridY;
+    CK(launch_plane(mode, c->az.lp, a, c->st));
+    c->launches++;
+  }
+  return prof_end(c, 10 + mode) ? -1 : 1;
+}
+
 // dst = B(M(F(src))) over the non-x axes, M applied in the last axis pass
 // (or pointwise if there is no other axis).  src may equal dst.
 int middle(spb_ctx *c, int mid_mode, const float2 *src, float2 *dst, PassArgs a) {
   int axes[2];
   const int k = other_axes(c, axes);
   if (k == 0) return col(c, 0, mid_mode, src, dst, a);
+  if (k == 2) {
+    const int pr = plane_pass(c, mid_mode, src, dst, a);
+    if (pr) return pr < 0 ? -1 : 0;
+  }
   const float2 *s = src;
   for (int i = 0; i < k - 1; i++) {
     if (col(c, axes[i], COL_FWD, s, dst, a)) return -1;

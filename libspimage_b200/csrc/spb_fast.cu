@@ -841,6 +841,109 @@ cudaError_t launch_persist(const LinePlan &px, const PassArgs &a, float2 *g0, fl
   return cudaErrorNotSupported;
 }
 
+// ------------------------------------------------- 3-D plane pass (ny = nz)
+// The y and z passes of a 3-D iteration in one launch: one block per x-plane
+// of a start holds the plane's N x N points (rows along y, one per z) in
+// shared memory and runs the forward y transforms (rows), then per column
+// (one per y) the forward z transform, the projection and the inverse z
+// transform, then the inverse y transforms (rows).  That is the work of the
+// forward y, z projection and inverse y column passes, with one read and one
+// write of the volume instead of three of each.  Same transforms, projection
+// and order, so the bits are those of the three passes.
+//
+// Shared memory: [twiddles N][N rows of pitch P = N + N/16] as in the
+// persistent form: point (z, y) of the plane at z*P + y; a row's exchanges
+// use the padded positions of its own P slots, a column's use its own
+// elements (stride P).  Plane loads and stores are 8-byte accesses at stride
+// nx points; the neighbouring planes' blocks run at the same time and share
+// the sectors in L2.
+template <int N, int MODE>
+__global__ void __launch_bounds__(N * N / 16, 1) plane_kernel(PassArgs a, const float2 *__restrict__ stw) {
+  constexpr int T = N / 16;
+  constexpr int P = N + N / 16;
+  constexpr int W = proj_words(N);
+  extern __shared__ __align__(16) float2 sm[];
+  float2 *tw_s = sm;
+  float2 *Ps = sm + N;
+  const int x = blockIdx.x;
+  const long long b = a.outer0 + blockIdx.y;
+  const long long nxy = (long long)a.nx * N;  // points per z-slice (ny = N)
+  const long long off = b * a.n_start + x;     // point (z, y) of the plane at off + z*nxy + y*nx
+  stage_twiddles<N>(tw_s, stw);
+  pdl_wait();
+  {  // forward y: row r (z = r), thread t of its T, straight from global memory
+    const int r = threadIdx.x / T, t = threadIdx.x % T;
+    const float2 *src = a.src + off + (long long)r * nxy + (long long)t * a.nx;
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = src[(long long)(T * q) * a.nx];
+    cp_async_wait_all();
+    __syncthreads();  // twiddles in
+    reg::PStages<N, 0, 1, false, 0>::run(v, Ps + r * P, t, tw_s);
+#pragma unroll
+    for (int q = 0; q < 16; q++) Ps[r * P + t + T * q] = v[q];
+    __syncthreads();
+  }
+  {  // column c (y = c), thread t of its T: forward z, projection, inverse z
+    const int c = threadIdx.x % N, t = threadIdx.x / N;
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = Ps[(t + T * q) * P + c];
+    __syncthreads();  // every column read before its elements serve as exchange space
+    reg::PStages<N, 0, 1, false, P>::run(v, Ps + c, t, tw_s);
+    const long long line = (long long)c * a.nx + x;  // z-line index y*nx + x
+    project16<T, MODE == COL_PROJECT>(v, a.amp_line + line * N, a.meas_bits + line * W, t,
+                                      (size_t)(off + (long long)c * a.nx + (long long)t * nxy), (size_t)T * nxy, a);
+    reg::PStages<N, 0, 1, true, P>::run(v, Ps + c, t, tw_s);
+#pragma unroll
+    for (int q = 0; q < 16; q++) Ps[(t + T * q) * P + c] = v[q];
+    __syncthreads();
+  }
+  {  // inverse y: row r, thread t
+    const int r = threadIdx.x / T, t = threadIdx.x % T;
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = Ps[r * P + t + T * q];
+    __syncthreads();  // every row read before its slots serve as exchange space
+    reg::PStages<N, 0, 1, true, 0>::run(v, Ps + r * P, t, tw_s);
+    pdl_release();
+    float2 *dst = a.dst + off + (long long)r * nxy + (long long)t * a.nx;
+#pragma unroll
+    for (int q = 0; q < 16; q++) dst[(long long)(T * q) * a.nx] = v[q];
+  }
+}
+
+template <int N, int MODE>
+static cudaError_t plane_launch_n(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+  const size_t smem = (size_t)(N + N * (N + N / 16)) * sizeof(float2);
+  cudaError_t e = ensure_smem<plane_kernel<N, MODE>>(smem);
+  if (e != cudaSuccess) return e;
+  return launch_maybe_pdl(plane_kernel<N, MODE>, dim3(a.nx, a.nouter), dim3(N * N / 16), smem, st, a.pdl != 0, a,
+                          pl.stw);
+}
+
+// Whether the plane pass serves this projection: a 3-D volume with ny = nz =
+// 64 or 128, a projection mode, the line-major amplitudes and measured bits.
+bool plane_fits(int mode, const LinePlan &pl, const PassArgs &a) {
+  if (mode != COL_PROJECT && mode != COL_PROJECT_NOFC) return false;
+  if (a.nz == 1 || pl.n != a.ny || a.ny != a.nz || (pl.n != 64 && pl.n != 128)) return false;
+  return pl.stw && a.amp_line && a.meas_bits && a.meas_words == proj_words(pl.n);
+}
+
+// The plane pass (cudaErrorNotSupported where plane_fits says no); a.nouter
+// starts from a.outer0 (at most 65535 per launch).
+cudaError_t launch_plane(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
+  if (!plane_fits(mode, pl, a)) return cudaErrorNotSupported;
+  switch (pl.n) {
+    case 64:
+      return mode == COL_PROJECT ? plane_launch_n<64, COL_PROJECT>(pl, a, st) : plane_launch_n<64, COL_PROJECT_NOFC>(pl, a, st);
+    case 128:
+      return mode == COL_PROJECT ? plane_launch_n<128, COL_PROJECT>(pl, a, st)
+                                 : plane_launch_n<128, COL_PROJECT_NOFC>(pl, a, st);
+  }
+  return cudaErrorNotSupported;
+}
+
 // ------------------------------------------- self-check of the roundings
 // Bit-for-bit comparisons of the branch-free forms with the IEEE intrinsics,
 // counting differences: every float x with bit pattern in [lo, hi) inside the

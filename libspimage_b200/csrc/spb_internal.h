@@ -130,6 +130,10 @@ bool col_width_ok(int n, int w);
 // all iterations of a call for every start of an N x N pattern (N = 32, 64,
 // 128), one block per start with its spectrum resident (spb_fast.cu); a.dst
 // holds X on entry and exit, g0/g1 are the two iterate buffers (start-major)
+// the y and z passes of a 3-D volume with ny = nz = 64 or 128 in one launch
+// (spb_fast.cu plane_kernel); cudaErrorNotSupported where it does not apply
+bool plane_fits(int mode, const LinePlan &pl, const PassArgs &a);
+cudaError_t launch_plane(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
 cudaError_t launch_persist(const LinePlan &px, const PassArgs &a, float2 *g0, float2 *g1, int cur0, int iters,
                            int keep_gp, int nb, cudaStream_t st);
 // 8-point kernels of the iteration's two passes (spb_split.cu)

@@ -40,7 +40,7 @@ def _margins(shape):
     return amp, mask, support, amin, amax
 
 
-@pytest.mark.parametrize("shape,alg", [((48, 40), HIO), ((64, 64), RAAR), ((8, 16, 12), ER)])
+@pytest.mark.parametrize("shape,alg", [((48, 40), HIO), ((64, 64), RAAR), ((8, 16, 12), ER), ((64, 64, 16), HIO)])
 def test_amplitude_margins_bit_exact(lib, oracle_mod, shape, alg):
     amp, mask, support, amin, amax = _margins(shape)
     engines = []

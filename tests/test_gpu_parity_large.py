@@ -285,3 +285,32 @@ def test_tma_projection_bit_exact(lib, oracle_mod, shape, alg, starts, tma):
         ref = setup_pattern(oracle_mod.Restatement(shape, threads=8), pat, alg, 0.87, sup, seed=30 + (k or 0))
         assert ref.iterate(23) == 0
         assert_same_state(gpu, ref, start=k)
+
+
+PLANE = 7  # tuning knob: 2 = the y and z parts of a 3-D iteration as one plane pass, 1 (or 0) = three column passes
+
+
+@pytest.mark.parametrize("shape,alg,starts,cons", [((64, 64, 32), HIO, None, 2), ((128, 128, 32), DIFFMAP, None, 2),
+                                                   ((64, 64, 16), RAAR, 3, 2 | 16), ((128, 128, 16), ER, None, 1)])
+def test_plane_pass_bit_exact(lib, oracle_mod, shape, alg, starts, cons):
+    """3-D volumes with ny = nz = 64 or 128: the plane pass (one block per
+    x-plane: forward y, forward z, projection, inverse z, inverse y) and the
+    three column passes it replaces both give the oracle's bits -- HIO, the
+    difference map (whose second projection has no Fourier constraints), a
+    batch of starts with centrosymmetry, ER with a real object."""
+    pat = synth.make_pattern(shape, min(shape) // 4, 1e7, min(shape) / 32.0, seed=12)
+    sup = [(AREA, 9, {0: 3.0, 60: 0.7}, 0.05)]
+    seeds = list(range(40, 40 + starts)) if starts else None
+    refs = {}
+    for plane in (2, 1):
+        gpu = setup_pattern(lib.Phaser(shape), pat, alg, 0.87, sup, constraints=cons, seed=40, starts=seeds)
+        gpu.set_tuning(PLANE, plane)
+        assert gpu.iterate(23) == 0
+        for k in ([0, starts - 1] if starts else [None]):
+            if k not in refs:
+                ref = setup_pattern(oracle_mod.Restatement(shape, threads=8), pat, alg, 0.87, sup, constraints=cons,
+                                    seed=40 + (k or 0))
+                assert ref.iterate(23) == 0
+                refs[k] = ref
+            assert_same_state(gpu, refs[k], start=k)
+        gpu.close()
