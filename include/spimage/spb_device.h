@@ -97,7 +97,9 @@ const char *spb_kernel_name(int kind);
  * column tiles -- 0 (the built-in choice) with the tensor memory accelerator
  * (bulk tensor loads under an mbarrier and bulk tensor stores) where the
  * tile fits and no other column width is asked for, 2 with it wherever the
- * tile fits, 1 with plain loads and stores; SPB_TUNE_PLANE: how a 3-D
+ * tile fits and, in addition, the HIO/RAAR/ER row pass with 1-D bulk copies
+ * of its rows (rows of 64 points or more; measured no faster than its plain
+ * coalesced loads), 1 with plain loads and stores; SPB_TUNE_PLANE: how a 3-D
  * volume with ny = nz = 64 or 128 runs the y and z parts of an iteration --
  * 2 as one plane pass (one block per x-plane: forward y, forward z,
  * projection, inverse z, inverse y; measured slower than the column passes

@@ -529,6 +529,24 @@ __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.p
 // polls of the tile's mbarrier before the block gives up (each try_wait may
 // suspend the thread for a while; a stuck copy ends the block within seconds)
 constexpr long long kTmaWaitPolls = 1LL << 22;
+
+// Waits for phase `parity` of the mbarrier with a bounded number of polls.
+// The answer is the block's (a barrier): false on every thread if any gave
+// up, so the block leaves together and no thread is left at a later barrier.
+__device__ __forceinline__ bool mbar_wait_block(uint64_t *bar, unsigned parity) {
+  bool ok = false;
+  for (long long i = 0; i < kTmaWaitPolls && !ok; i++) ok = mbar_try_wait(bar, parity);
+  return !__syncthreads_or(!ok);
+}
+
+// 1-D bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned)
+// from global to shared memory, completing on the mbarrier's byte count
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"((unsigned long long)src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
 // shared-memory alignment of the bulk tensor copies' boxes (bytes)
 constexpr unsigned kTmaSmemAlign = 128;
 
@@ -594,10 +612,8 @@ __global__ void __launch_bounds__(256) col_tma_kernel(PassArgs a, const float2 *
 #pragma unroll
     for (int k = 0; k < N / BOX; k++) tma_load_2d(tile + k * BOX * C, &tin, col0, (int)(o * N + k * BOX), &bar);
   }
-  bool ok = false;
-  for (long long i = 0; i < kTmaWaitPolls && !ok; i++) ok = mbar_try_wait(&bar, 0);
-  if (!ok) {  // the tile never arrived: flag it and leave (nothing of this block is written)
-    if (a.err_flag) atomicExch(a.err_flag, 1);
+  if (!mbar_wait_block(&bar, 0)) {  // the tile never arrived: flag it and leave (nothing of this block is written)
+    if (threadIdx.x == 0 && a.err_flag) atomicExch(a.err_flag, 1);
     return;
   }
   float2 v[16];
@@ -676,6 +692,126 @@ static cudaError_t col_tma_launch(const LinePlan &pl, const PassArgs &a, cudaStr
   if (e != cudaSuccess) return e;
   dim3 grid((a.ncols + C - 1) / C, a.nouter);
   return launch_maybe_pdl(col_tma_kernel<N, MODE, C>, grid, dim3(C * T), smem, st, a.pdl != 0, a, pl.stw, tin, tout);
+}
+
+// --------------------------------------- iteration row pass staged by TMA
+// The row pass of an HIO/RAAR/ER iteration (row_fast_kernel<N, ROW_ITER,
+// G0LATE>) with its inputs moved by 1-D bulk copies: one thread arms an
+// mbarrier with the block's byte count and copies each row's flags (and,
+// unless G0LATE, its previous iterate) before the dependent-launch wait --
+// they were written two or more kernels earlier -- and each row of Y after
+// it, dense into the row's exchange line, which is free before the first
+// stage.  With G0LATE the previous iterate's rows are copied into the
+// exchange lines between the two transforms under a second mbarrier.  The
+// transforms, the update and the outputs are those of row_fast_kernel, so
+// the bits are too.  Rows of N >= 64 points: every row, line and flag row
+// starts on a 16-byte boundary and is a multiple of 16 bytes long.
+template <int N, bool G0LATE>
+__global__ void __launch_bounds__(256) row_tma_kernel(PassArgs a, const float2 *__restrict__ stw, int nrows) {
+  constexpr int T = N / 16;
+  constexpr int S = N + N / 16;
+  static_assert(N >= 64 && (S * sizeof(float2)) % 16 == 0 && N % 16 == 0, "rows and lines of whole 16-byte chunks");
+  extern __shared__ __align__(16) float2 sm[];
+  __shared__ __align__(8) uint64_t bar[2];
+  const int lpb = blockDim.x / T;
+  const int lr = threadIdx.x / T, t = threadIdx.x % T;
+  const int row0 = blockIdx.x * lpb;
+  const int row = row0 + lr;
+  const bool valid = row < nrows;
+  float2 *tw_s = sm;
+  float2 *line = sm + N + lr * S;
+  const size_t base = (size_t)row * N + t;
+  float2 *g0_s = sm + N + lpb * S;  // an even float2 offset: 16-byte aligned
+  uint8_t *fl_s = reinterpret_cast<uint8_t *>(g0_s + (G0LATE ? 0 : lpb * N));
+  const int vrows = min(lpb, nrows - row0);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  stage_twiddles<N>(tw_s, stw);
+  __syncthreads();  // the barriers' initialisation before any copy or wait
+  if (threadIdx.x == 0) {
+    const unsigned per_row = N * (unsigned)(sizeof(float2) + 1 + (G0LATE ? 0 : sizeof(float2)));
+    mbar_expect_tx(&bar[0], per_row * (unsigned)vrows);
+    for (int r = 0; r < vrows; r++) bulk_load(fl_s + r * N, a.flags + (size_t)(row0 + r) * N, N, &bar[0]);
+    if constexpr (!G0LATE)
+      for (int r = 0; r < vrows; r++)
+        bulk_load(g0_s + r * N, a.g0 + (size_t)(row0 + r) * N, N * (unsigned)sizeof(float2), &bar[0]);
+  }
+  pdl_wait();
+  if (threadIdx.x == 0)
+    for (int r = 0; r < vrows; r++)
+      bulk_load(sm + N + r * S, a.src + (size_t)(row0 + r) * N, N * (unsigned)sizeof(float2), &bar[0]);
+  if (!mbar_wait_block(&bar[0], 0)) {  // the rows never arrived: flag it and leave (nothing is written)
+    if (threadIdx.x == 0 && a.err_flag) atomicExch(a.err_flag, 1);
+    return;
+  }
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) v[q] = valid ? line[t + T * q] : make_float2(0.0f, 0.0f);
+  cp_async_wait_all();  // twiddles
+  __syncthreads();      // every row read before the exchanges reuse the lines
+  const float beta = iter_beta(a);
+  const float one_m2b = fsub(1.0f, fmul(2.0f, beta));  // 1 - 2*beta in float, as the reference
+  reg::fft<N, true>(v, line, t, tw_s);
+  if constexpr (G0LATE) {
+    // the transform's last stage uses registers only and a barrier followed
+    // its last exchange: the lines are free for the previous iterate
+    if (threadIdx.x == 0) {
+      fence_proxy_async_smem();
+      mbar_expect_tx(&bar[1], (unsigned)vrows * N * (unsigned)sizeof(float2));
+      for (int r = 0; r < vrows; r++)
+        bulk_load(sm + N + r * S, a.g0 + (size_t)(row0 + r) * N, N * (unsigned)sizeof(float2), &bar[1]);
+    }
+    if (!mbar_wait_block(&bar[1], 0)) {
+      if (threadIdx.x == 0 && a.err_flag) atomicExch(a.err_flag, 1);
+      return;
+    }
+  }
+  const float2 *g0r = G0LATE ? line + t : g0_s + lr * N + t;
+  const uint8_t *flr = fl_s + lr * N + t;
+  float2 *gp = a.gp;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    float2 g = make_float2(0.0f, 0.0f);
+    if (valid) {
+      const float2 gpv = scale_cmul_dev(v[q], a.inv_n);
+      if (gp) gp[base + T * q] = gpv;
+      const uint8_t f = flr[T * q];
+      if (f & FLAG_INSIDE) {
+        g = gpv;
+      } else if (a.alg == ALG_HIO) {
+        const float2 g0 = g0r[T * q];
+        g = make_float2(fsub(g0.x, fmul(gpv.x, beta)), fsub(g0.y, fmul(gpv.y, beta)));
+      } else if (a.alg == ALG_RAAR) {
+        const float2 g0 = g0r[T * q];
+        g = make_float2(fadd(fmul(gpv.x, one_m2b), fmul(g0.x, beta)), fadd(fmul(gpv.y, one_m2b), fmul(g0.y, beta)));
+      }
+      g = apply_constraints(g, f, a.constraints);
+      a.g1[base + T * q] = g;
+    }
+    v[q] = g;
+  }
+  if constexpr (G0LATE) __syncthreads();  // every g0 read done before the forward transform writes the lines
+  reg::fft<N, false>(v, line, t, tw_s);
+  pdl_release();
+  if (valid)
+#pragma unroll
+    for (int q = 0; q < 16; q++) a.dst[base + T * q] = v[q];
+}
+
+// Whether the TMA row pass serves this launch: rows of 64..4096 points whose
+// buffers start on 16-byte boundaries (every row then does too).  It runs
+// only when asked for (SPB_TUNE_TMA = 2): measured on one B200 (graph-
+// replayed calls, us per slot, plain / TMA rows) RAAR 1024^2 19.1-19.3 /
+// 20.1-20.2, HIO 256^2 9.84 / 9.83, 512 starts of 512^2 1531-1547 /
+// 1546-1548, HIO 128^3 40.2 / 40.9 -- the plain rows are coalesced 256-byte
+// warp loads already, and the block waits for all of its rows either way.
+template <int N>
+static bool row_tma_fits(const PassArgs &a) {
+  if (N < 64) return false;
+  return !(((uintptr_t)a.src | (uintptr_t)a.g0 | (uintptr_t)a.flags) & 15);
 }
 
 // ------------------------------------------------ persistent small patterns
@@ -1049,6 +1185,21 @@ static cudaError_t row_fast_launch(const LinePlan &px, const PassArgs &a, cudaSt
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, row_fast_kernel<N, MODE, false>, LPB * T, smem_early);
       if (e != cudaSuccess) return e;
       late = grid > (long long)per_sm * nsm;
+    }
+    if constexpr (MODE == ROW_ITER && N >= 64) {
+      // the rows staged by TMA (knob 2; same shared memory as the plain form)
+      if (a.tma == 2 && row_tma_fits<N>(a)) {
+        if (late) {
+          cudaError_t e = ensure_smem<row_tma_kernel<N, true>>(smem_late);
+          if (e != cudaSuccess) return e;
+          return launch_maybe_pdl(row_tma_kernel<N, true>, dim3((unsigned)grid), dim3(LPB * T), smem_late, st,
+                                  a.pdl != 0, a, px.stw, (int)nrows);
+        }
+        cudaError_t e = ensure_smem<row_tma_kernel<N, false>>(smem_early);
+        if (e != cudaSuccess) return e;
+        return launch_maybe_pdl(row_tma_kernel<N, false>, dim3((unsigned)grid), dim3(LPB * T), smem_early, st,
+                                a.pdl != 0, a, px.stw, (int)nrows);
+      }
     }
     if (late) {
       cudaError_t e = ensure_smem<row_fast_kernel<N, MODE, true>>(smem_late);

@@ -273,7 +273,10 @@ def test_tma_projection_bit_exact(lib, oracle_mod, shape, alg, starts, tma):
     """The projection pass with its column tiles moved by bulk tensor copies
     (TMA, the built-in choice where the tile fits) and with plain loads and
     stores gives the oracle's bits: 2-D y lines, 3-D z lines (tile rows of
-    64*64 points), and 64-point columns of 1008-point rows."""
+    64*64 points), and 64-point columns of 1008-point rows.  With knob 2 the
+    iteration's row pass moves its rows by bulk copies too (HIO/RAAR/ER rows
+    of 64 points or more; the previous iterate staged up front for single
+    patterns, between the transforms for the 8-start batch)."""
     pat = synth.make_pattern(shape, min(shape) // 4, 1e7, min(shape) / 32.0, seed=9)
     sup = [(AREA, 9, {0: 3.0, 60: 0.7}, 0.05)]
     seeds = list(range(30, 30 + starts)) if starts else None
