@@ -541,6 +541,15 @@ def summarise(rows):
             "queue_wait_p50_s": round(_pct(adm - sub, 50), 4), "queue_wait_p99_s": round(_pct(adm - sub, 99), 4)}
 
 
+def tune_alone(Server, warm, patterns):
+    """Runs the warm-up jobs one at a time: the server tunes the launch shapes
+    of every new (shape, starts, algorithm) on its first job, and the choice
+    is cached for the process -- timed with the GPU otherwise idle rather
+    than beside the other jobs of a concurrent warm-up."""
+    with Server(max_active_jobs=1, chunk_slots=100) as srv:
+        run_jobs(srv, warm, [0.0] * len(warm), patterns)
+
+
 def mixed_run(args, L):
     """Uneven mixed batch: single-start jobs of 2-D sizes drawn from
     {128, 192, 256, 384, 512, 1000}^2 with a random algorithm and beta, plus
@@ -564,11 +573,13 @@ def mixed_run(args, L):
     for j in jobs:
         patterns.get(j["shape"], j["pattern"])
     res = {}
+    # warm-up: one short job per shape and algorithm (launch-shape tuning,
+    # module loading, graph capture)
+    warm = [{"shape": sh, "stages": [(a, 0.9, 40)], "starts": 1, "seed": 0, "period": 20, "pattern": 0}
+            for sh in MIXED_SIZES + [(128, 128, 128)] for a in (1, 2, 3, 4)]
+    tune_alone(Server, warm, patterns)
     for label, active in (("concurrent", args.max_active_jobs), ("one_at_a_time", 1)):
         with Server(max_active_jobs=active, chunk_slots=100) as srv:
-            # warm-up: one short job per shape and algorithm (module loading, graph capture)
-            warm = [{"shape": sh, "stages": [(a, 0.9, 40)], "starts": 1, "seed": 0, "period": 20, "pattern": 0}
-                    for sh in MIXED_SIZES + [(128, 128, 128)] for a in (1, 2, 3, 4)]
             run_jobs(srv, warm, [0.0] * len(warm), patterns)
             rows = run_jobs(srv, jobs, [0.0] * len(jobs), patterns)
             res[label] = summarise(rows)
@@ -614,11 +625,13 @@ def serving_run(args, L):
                        "100 ER) per job, area support every 20; sizes 128^2 .30, 256^2 .30, 512^2 .20, "
                        "1024^2 .15, 128^3 .05",
            "unit": "jobs/s", "max_active_jobs": args.max_active_jobs}
+    warm, _ = make_jobs(50.0, 0.2, 99)
+    warm = [dict(j, stages=[(HIO_, 0.9, 40), (ER_, 0.0, 10)]) for j in warm]
+    warm += [{"shape": sh, "stages": [(HIO_, 0.9, 40), (ER_, 0.0, 10)], "starts": 8, "seed": 0, "period": 20,
+              "pattern": 0} for sh, _ in SERVE_SIZES]
+    tune_alone(Server, [{"shape": sh, "stages": [(HIO_, 0.9, 40), (ER_, 0.0, 10)], "starts": 8, "seed": 0,
+                         "period": 20, "pattern": 0} for sh, _ in SERVE_SIZES], patterns)
     with Server(max_active_jobs=args.max_active_jobs, chunk_slots=100) as srv:
-        warm, _ = make_jobs(50.0, 0.2, 99)
-        warm = [dict(j, stages=[(HIO_, 0.9, 40), (ER_, 0.0, 10)]) for j in warm]
-        warm += [{"shape": sh, "stages": [(HIO_, 0.9, 40), (ER_, 0.0, 10)], "starts": 8, "seed": 0, "period": 20,
-                  "pattern": 0} for sh, _ in SERVE_SIZES]
         run_jobs(srv, warm, [0.0] * len(warm), patterns)
         # offered load at the configured rate (far above capacity): queueing-dominated
         jobs, arr = make_jobs(args.serve_rate, args.serve_window, 0)

@@ -92,7 +92,9 @@ const char *spb_kernel_name(int kind);
  * 0 the built-in choice (persistent for 32x32 and 64x64 patterns with at
  * least one start per SM); SPB_TUNE_COL_WIDTH = columns per block of the
  * projection pass along the last axis, for lines of 256 (1..16 columns),
- * 512 (1..8) or 1024 (1..4) points; 0 the built-in width; SPB_TUNE_TMA:
+ * 512 (1..8) or 1024 (1..4) points, and of the general kernels' lengths 192
+ * (1..16), 384 (1..8) and 1000 (1..4); powers of two; 0 the built-in width;
+ * SPB_TUNE_TMA:
  * how the projection pass of 16-point lines of 64 points or more moves its
  * column tiles -- 0 (the built-in choice) with the tensor memory accelerator
  * (bulk tensor loads under an mbarrier and bulk tensor stores) where the

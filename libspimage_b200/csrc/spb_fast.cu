@@ -1244,10 +1244,11 @@ static cudaError_t col_fast_launch_p(const LinePlan &pl, const PassArgs &a, cuda
 
 // Columns per block the projection pass offers besides the built-in width:
 // lines of 256, 512 and 1024 points, C a power of two with C*N/16 <= 256
-// threads and C <= 16 (the shared-memory skew is 16/C words).
+// threads and C <= 16 (the shared-memory skew is 16/C words); and the
+// lengths the general kernels run with compile-time plans (general_col_width_ok).
 bool col_width_ok(int n, int w) {
   if (w < 1 || w > 16 || (w & (w - 1))) return false;
-  if (n != 256 && n != 512 && n != 1024) return false;
+  if (n != 256 && n != 512 && n != 1024) return general_col_width_ok(n, w);
   return w * (n / 16) <= 256;
 }
 

@@ -127,6 +127,8 @@ cudaError_t launch_row_fast(int mode, const LinePlan &px, const PassArgs &a, cud
 cudaError_t launch_col_fast(int mode, const LinePlan &pl, const PassArgs &a, cudaStream_t st);
 // whether the projection pass has a kernel of w columns per block for lines of n points
 bool col_width_ok(int n, int w);
+// the same for the general kernels' compile-time-plan lengths (192, 384, 1000)
+bool general_col_width_ok(int n, int w);
 // all iterations of a call for every start of an N x N pattern (N = 32, 64,
 // 128), one block per start with its spectrum resident (spb_fast.cu); a.dst
 // holds X on entry and exit, g0/g1 are the two iterate buffers (start-major)

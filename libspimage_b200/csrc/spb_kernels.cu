@@ -361,17 +361,41 @@ cudaError_t launch_row(int mode, const LinePlan &px, const PassArgs &a, cudaStre
   return cudaErrorInvalidValue;
 }
 
+// Columns per block SPB_TUNE_COL_WIDTH may ask of the general projection pass
+// for the compile-time-plan lengths: a power of two up to 16 that keeps one
+// butterfly per thread within 1024 threads.
+bool general_col_width_ok(int n, int w) {
+  if (w < 1 || w > 16 || (w & (w - 1))) return false;
+  switch (n) {
+#define SPB_CASE(len) \
+  case len: return w * ct_max_butterflies(len) <= 1024;
+    SPB_CT_LENGTHS(SPB_CASE)
+#undef SPB_CASE
+  }
+  return false;
+}
+
 template <int MODE, int NC>
 static cudaError_t col_launch_n(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
   const int n = pl.n;
+  constexpr bool PROJ = (MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC);
   int ct = 4096 / (n > 0 ? n : 1);
   if (ct > 16) ct = 16;
   if (ct < 1) ct = 1;
   int tpc = NC > 0 ? ct_max_butterflies(NC) : pow2_at_least((n + 15) / 16);
   if (NC > 0 && tpc * ct > 1024) ct = 1024 / tpc > 0 ? 1024 / tpc : 1;  // keep one butterfly per thread
+  // projection with a compile-time plan: four columns per block (a full
+  // 32-byte sector per row, and more blocks than the wider default gives a
+  // single pattern).  Measured on one B200, HIO per slot at 16/8/4/2/1 columns:
+  // 192^2 13.6/12.2/11.6/11.9/12.6 us, 384^2 -/16.4/14.9/15.9/17.8 us, 1000^2
+  // (four by default) 39.2, 49.2 at 2, 57.7 at 1.  A launch-shape knob may
+  // ask for another number of columns per block.
+  if (NC > 0 && PROJ) {
+    if (ct > 4) ct = 4;
+    if (a.col_width > 0 && general_col_width_ok(NC, a.col_width)) ct = a.col_width;
+  }
   if (tpc * ct > 1024) tpc = 1024 / ct;
   if (tpc * ct < 32) tpc = 32 / ct;
-  constexpr bool PROJ = (MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC);
   // two transform buffers, then (projection) n*ct amplitudes and n*ct flag
   // bytes, then (compile-time plans) the n - 1 entries of the stage table
   const size_t smem = NC > 0 ? col_tw_offset(n, ct, PROJ) + (size_t)(NC - 1) * sizeof(float2)

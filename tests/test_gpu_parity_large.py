@@ -245,10 +245,12 @@ COL_WIDTH = 5  # tuning knob: columns per block of the projection pass
 
 
 @pytest.mark.parametrize("shape,widths", [((256, 64), (1, 2, 4, 8, 16)), ((512, 96), (1, 2, 4, 8)),
-                                          ((1024, 32), (1, 2, 4))])
+                                          ((1024, 32), (1, 2, 4)), ((192, 48), (1, 2, 4, 8, 16)),
+                                          ((384, 40), (1, 2, 4, 8)), ((1000, 24), (1, 2, 4))])
 def test_projection_column_widths_bit_exact(lib, oracle_mod, shape, widths):
     """Every columns-per-block shape of the projection pass the autotuner can
-    choose gives the oracle's bits."""
+    choose gives the oracle's bits: the register kernels' 256/512/1024-point
+    columns and the general kernels' 192/384/1000-point ones."""
     pat = synth.make_pattern(shape, min(shape) // 4, 1e7, min(shape) / 32.0, seed=8)
     sup = [(AREA, 9, 2.0, 0.1)]
     ref = setup_pattern(oracle_mod.Restatement(shape, threads=8), pat, RAAR, 0.87, sup, seed=3)
