@@ -709,15 +709,17 @@ static int upload(spb_ctx *c, void *dst, const void *src, size_t bytes) {
   return 0;
 }
 
-// after the context's stream has drained: a kernel whose bounded wait ran
-// out (a tile that never arrived) has set the error flag
+// after the context's stream has drained: a TMA pass kernel whose bounded
+// wait ran out (a tile or row that never arrived: 1) or whose tile was
+// misaligned (2) has set the error flag; it stays set (the results are not
+// to be trusted again)
 static int check_err_flag(spb_ctx *c) {
   if (c->tune[SPB_TUNE_TMA] == 1) return 0;  // no TMA pass runs
   int h = 0;
   CK(cudaMemcpyAsync(&h, c->err_flag, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   if (h == 2) return fail("a TMA pass kernel found its shared-memory tile or first column misaligned and copied nothing: results are invalid");
-  if (h) return fail("a pass kernel gave up waiting for its tile (bounded mbarrier wait): results are invalid");
+  if (h) return fail("a TMA pass kernel gave up waiting for its tile or rows (bounded mbarrier wait): results are invalid");
   return 0;
 }
 
