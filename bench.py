@@ -868,6 +868,7 @@ def reference_arm(args):
     total = float(sum(times))
     value = args.steps * sample / total
     modes = cpu_modes(args.workload, sample, 40)
+    ref_gpu = reference_cuda_engine(wl, args.workload)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3),
@@ -879,8 +880,55 @@ def reference_arm(args):
                                    "the oracle CPU FFT (no libfftw3f on the box)",
                          "mode": "iii_one_job_all_threads", "modes": modes},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda_engine": ref_gpu,
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_cuda_engine(wl, wl_name, slots=520):
+    """The reference's own CUDA engine (its phasing.cu kernels over cuFFT,
+    cuRAND and thrust, compiled for sm_100a into oracle/_ref) on a bounded
+    sample of the same workload on GPU 0: a second baseline beside the CPU
+    engine.  Wall clock with the device synchronised (the engine works on the
+    legacy default stream and synchronises inside its support updates)."""
+    import oracle
+
+    if not oracle.ref_cuda_available():
+        return {"unavailable": "oracle/_ref/libspref_cuda.so is not built (needs the reference sources and nvcc)"}
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        from libspimage_b200 import synth
+
+        amp, mask, support, _ = synth.workload(wl["pattern"], seed=0)
+        e = oracle.ReferenceCuda(wl["shape"])
+        name, beta, _ = wl["stages"][0]
+        e.set_algorithm({"HIO": oracle.HIO, "RAAR": oracle.RAAR, "ER": oracle.ER, "DM": oracle.DIFFMAP}[name],
+                        beta=beta if beta is not None else 0.9, constraints=wl["constraints"])
+        e.add_support_update(oracle.SUP_AREA, wl["period"], wl["blur"], wl["area"])
+        if e.start() != 0:
+            return {"unavailable": "sp_phaser_init with the reference's CUDA engine failed"}
+        e.set_amplitudes(amp, mask)
+        e.init_model(oracle.RANDOM_PHASES, seed=0)
+        e.set_support(support)
+        e.iterate(2 * wl["period"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = e.iterate(slots)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if rc != 0:
+            return {"unavailable": f"the reference's CUDA engine returned {rc}"}
+        return {"value": round(slots / dt, 3), "unit": UNIT, "us_per_slot": round(dt / slots * 1e6, 2),
+                "sample": f"{slots} iteration slots of the first stage ({name}) of {wl_name}, support updates "
+                          "included, after a warm-up of two support periods",
+                "engine": "the reference's CUDA engine (src/phasing.cu, phasing_kernels.cu, support_update_cuda.cu, "
+                          "image_filter_cuda.cu, fft.cu over cuFFT, cuRAND and thrust) compiled unmodified for sm_100a",
+                "efourier_after": e.efourier()[0]}
+    except Exception as ex:  # a baseline: report, do not fail the arm
+        return {"unavailable": f"{type(ex).__name__}: {ex}"[:300]}
 
 
 def main():

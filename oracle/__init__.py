@@ -29,6 +29,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATE_SO = os.path.join(HERE, "build", "libsporacle.so")
 REF_SO = os.path.join(HERE, "_ref", "libspref.so")
+# the reference's CUDA engine (cuFFT, cuRAND, thrust), built by `make refcuda`
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libspref_cuda.so")
 
 HIO, RAAR, DIFFMAP, ER = 1, 2, 3, 4
 SUP_THRESHOLD, SUP_AREA, SUP_CENTRE, SUP_TEMPLATE, SUP_STATIC, SUP_CLOSE = 1, 2, 3, 4, 5, 6
@@ -59,12 +61,18 @@ def reference_root():
 
 
 def build(ref: bool = False) -> None:
-    """Compile the restatement (and the reference build when ``ref``)."""
+    """Compile the restatement (and the reference builds when ``ref``: its
+    CPU engine, and its CUDA engine where nvcc, cuFFT and cuRAND are at hand --
+    a baseline only, so a failure there is reported and not raised)."""
     target = ["all", "ref"] if ref else ["all"]
     extra = []
     if ref and os.environ.get("SPIMAGE_REFERENCE"):
         extra = [f"REF={os.environ['SPIMAGE_REFERENCE']}"]
     subprocess.run(["make", "-s", "-C", HERE] + target + extra, check=True)
+    if ref:
+        r = subprocess.run(["make", "-s", "-C", HERE, "refcuda"] + extra, capture_output=True, text=True)
+        if r.returncode != 0:
+            print("oracle: the reference's CUDA engine was not built:\n" + r.stderr[-2000:])
 
 
 def ref_available() -> bool:
@@ -135,13 +143,13 @@ def _load_restatement():
         return lib
 
 
-def _load_reference():
+def _load_reference(path=REF_SO):
     with _lock:
-        if "ref" in _libs:
-            return _libs["ref"]
-        if not os.path.exists(REF_SO):
-            raise RuntimeError("oracle/_ref/libspref.so is not built (needs the reference sources)")
-        lib = C.CDLL(REF_SO)
+        if path in _libs:
+            return _libs[path]
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle/_ref/{os.path.basename(path)} is not built (needs the reference sources)")
+        lib = C.CDLL(path)
         lib.ref_image_alloc.restype = _vp
         lib.ref_image_alloc.argtypes = [C.c_int, C.c_int, C.c_int]
         lib.ref_image_free.argtypes = [_vp]
@@ -218,7 +226,7 @@ def _load_reference():
         lib.sp_image_ifftw3.argtypes = [_vp]
         lib.sp_init_fft.restype = C.c_int
         lib.sp_init_fft.argtypes = [C.c_int]
-        _libs["ref"] = lib
+        _libs[path] = lib
         return lib
 
 
@@ -502,6 +510,40 @@ class Reference(_Engine):
 
     def support_fraction(self):
         return float(self.lib.sp_phaser_support_fraction(self.ph))
+
+
+def ref_cuda_available() -> bool:
+    return os.path.exists(REF_CUDA_SO)
+
+
+class ReferenceCuda(Reference):
+    """The reference's own CUDA engine (oracle/_ref/libspref_cuda.so: its
+    phasing.cu and friends over cuFFT, cuRAND and thrust, compiled for
+    sm_100a), driven through its C API with SpEngineCUDA.  A baseline to time
+    beside this project's kernels: its random starts come from cuRAND and its
+    transforms from cuFFT, so its iterates are not the CPU engine's bits.  The
+    model is read with sp_phaser_model (the engine keeps it on the device)."""
+
+    def __init__(self, shape):
+        _Engine.__init__(self, shape)
+        self.lib = _load_reference(REF_CUDA_SO)
+        self.lib.sp_phaser_model.restype = _vp
+        self.lib.sp_phaser_model.argtypes = [_vp]
+        self.ph = self.lib.sp_phaser_alloc()
+        self.alg = None
+        self.sup = None
+        self.images = []
+        self.amp_img = None
+        self.objective = 0
+
+    def start(self):
+        """sp_phaser_init with the CUDA engine; call after set_algorithm/add_support_update."""
+        return self.lib.sp_phaser_init(self.ph, self.alg, self.sup, 2)
+
+    def model(self):
+        img = self.lib.sp_phaser_model(self.ph)
+        d = np.ctypeslib.as_array(self.lib.ref_image_data(img), shape=(self.n * 2,)).copy().view(np.complex64)
+        return d.reshape(self.out_shape)
 
 
 def fft(x, sign=-1):
