@@ -202,6 +202,18 @@ int spb_ctx_get_start_flags(spb_ctx *ctx, int start, int *flags);
 int spb_ctx_set_start_model(spb_ctx *ctx, int start, const float *model, int reset_others);
 /* fourier holds nb spectra, start-major: g1[b] = IFFT(fourier[b])/N */
 int spb_ctx_models_from_fourier(spb_ctx *ctx, const float *fourier, int reset_others);
+/* Random-phase starts from their phases (no reference counterpart; the
+ * device form of sp_image_rephase followed by the inverse transform of
+ * sp_phaser_init_model, src/image_util.c:1035-1067 and src/phasing.c:606-650):
+ * g1[b] = IFFT(F_b)/N with F_b[i] = (cos(phase) |amp[i]|, sin(phase) |amp[i]|)
+ * evaluated in double and rounded to float as the reference does, phase =
+ * phases[i] (one = 1: the same phases for every start) or phases[b*N + i]
+ * (one = 0).  amp is the host copy of the amplitudes the context holds.  The
+ * device evaluates the trigonometry; the few elements whose float rounding
+ * could depend on the last bits of cos or sin (a product within 16 ulps of
+ * a float rounding midpoint) are evaluated on the host with the C library,
+ * so the result is the reference's bit for bit. */
+int spb_ctx_models_from_phases(spb_ctx *ctx, const float *phases, const float *amp, int one, int reset_others);
 /* g1[b] = IFFT(amp * exp(2 pi i u))/N with u drawn on the device by
  * Philox4x32-10 keyed by seeds[b] (throughput runs; the host API's
  * SpModelRandomPhases reproduces the reference's rand() stream instead) */

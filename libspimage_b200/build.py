@@ -24,7 +24,7 @@ LIB = os.path.join(PKG, "libspimage_b200.so")
 CU_SOURCES = ["spb_kernels.cu", "spb_fast.cu", "spb_split.cu", "spb_capi.cu"]
 C_SOURCES = ["host/image.c", "host/phasing.c", "host/support_update.c", "host/fft.c", "host/prtf.c"]
 CXX_SOURCES = ["host/serve.cpp"]
-HEADERS = ["spb_fft.cuh", "spb_internal.h", "spb_pointwise.cuh", "spb_passes.cuh"]
+HEADERS = ["spb_fft.cuh", "spb_internal.h", "spb_pointwise.cuh", "spb_passes.cuh", "host/host_internal.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xptxas", "-O3"]

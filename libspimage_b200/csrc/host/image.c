@@ -14,6 +14,7 @@
 #include <unistd.h>
 
 #include "spimage.h"
+#include "host_internal.h"
 
 sp_3matrix *_sp_3matrix_alloc(unsigned int nx, unsigned int ny, unsigned int nz, const char *file, int line) {
   (void)file; (void)line;
@@ -294,6 +295,59 @@ static void rephase_parallel(Complex *data, const uint32_t *w, long long n) {
     if (started[t]) pthread_join(th[t], NULL);
     else rephase_worker(&span[t]); /* no thread: do the span here */
   }
+}
+
+/* The phases alone: phase[i] = p_drand48() * 2 pi rounded to float, from the
+ * same rand() words, in the same pixel order, leaving the generator where n
+ * calls of rand() leave it -- the phases sp_image_rephase(SP_RANDOM_PHASE)
+ * would use for an image of n pixels (drawn on all host threads). */
+typedef struct {
+  float *phase;
+  const uint32_t *w;
+  long long i0, i1;
+} phase_span;
+
+static void *phase_worker(void *arg) {
+  const phase_span *s = (const phase_span *)arg;
+  uint32_t buf[RNG_DEG];
+  rng_window_at(s->w, s->i0, buf);
+  int f = 0, r = RNG_DEG - RNG_SEP;
+  for (long long i = s->i0; i < s->i1; i++) {
+    const uint32_t val = buf[f] + buf[r];
+    buf[f] = val;
+    f = f + 1 == RNG_DEG ? 0 : f + 1;
+    r = r + 1 == RNG_DEG ? 0 : r + 1;
+    const real u = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
+    s->phase[i] = u * 3.14159265358979323846 * 2;
+  }
+  return NULL;
+}
+
+void spb_random_phases(float *phase, long long n) {
+  uint32_t w[RNG_DEG];
+  if (n > 0 && rng_take(n, w)) {
+    long long nt = n >= (1 << 18) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
+    if (nt < 1) nt = 1;
+    if (nt > REPHASE_MAX_THREADS) nt = REPHASE_MAX_THREADS;
+    pthread_t th[REPHASE_MAX_THREADS];
+    phase_span span[REPHASE_MAX_THREADS];
+    int started[REPHASE_MAX_THREADS] = {0};
+    for (long long t = 0; t < nt; t++) {
+      span[t].phase = phase;
+      span[t].w = w;
+      span[t].i0 = n * t / nt;
+      span[t].i1 = n * (t + 1) / nt;
+      if (t > 0) started[t] = pthread_create(&th[t], NULL, phase_worker, &span[t]) == 0;
+    }
+    phase_worker(&span[0]);
+    for (long long t = 1; t < nt; t++) {
+      if (started[t]) pthread_join(th[t], NULL);
+      else phase_worker(&span[t]);
+    }
+    return;
+  }
+  /* another generator layout: one rand() per pixel */
+  for (long long i = 0; i < n; i++) phase[i] = p_drand48() * 3.14159265358979323846 * 2;
 }
 
 void sp_image_rephase(Image *img, int type) {

@@ -15,6 +15,7 @@
 
 #include "spimage.h"
 #include "spimage/spb_device.h"
+#include "host_internal.h"
 
 typedef struct {
   spb_ctx *ctx;
@@ -420,6 +421,17 @@ int sp_phaser_init_model(SpPhaser *ph, const Image *user_model, int flags) {
   int rc = 0;
   if (user_model) {
     rc = spb_ctx_set_model(ctx, (const float *)user_model->image->data, 1);
+  } else if (flags & SpModelRandomPhases) {
+    /* the phases from rand() on the host, the trigonometry on the device */
+    if (!ph->amplitudes) {
+      snprintf(g_last_err, sizeof(g_last_err), "sp_phaser_init_model: set the amplitudes before a random-phase start");
+      return -3;
+    }
+    float *phases = (float *)malloc(sizeof(float) * (size_t)ph->image_size);
+    if (!phases) return -8;
+    spb_random_phases(phases, ph->image_size);
+    rc = spb_ctx_models_from_phases(ctx, phases, ph->amplitudes->data, 1, 1);
+    free(phases);
   } else {
     Image *m = sp_image_alloc(ph->nx, ph->ny, ph->nz);
     if (draw_start(ph, flags, m)) rc = spb_ctx_model_from_fourier(ctx, (const float *)m->image->data, 1);
@@ -491,7 +503,21 @@ int sp_phaser_init_models(SpPhaser *ph, int flags, const int *seeds) {
   const size_t n = (size_t)ph->image_size;
   Image *m = sp_image_alloc(ph->nx, ph->ny, ph->nz);
   int rc = 0;
-  if (flags & (SpModelRandomPhases | SpModelZeroPhases)) {
+  if (flags & SpModelRandomPhases) {
+    /* nb starts' phases from rand() on the host (start b after sp_srand(seeds[b])),
+       the trigonometry and the transforms on the device */
+    float *phases = (float *)malloc(sizeof(float) * n * (size_t)nb);
+    if (!phases) {
+      sp_image_free(m);
+      return -8;
+    }
+    for (int b = 0; b < nb; b++) {
+      if (seeds) sp_srand(seeds[b]);
+      spb_random_phases(phases + n * (size_t)b, (long long)n);
+    }
+    rc = spb_ctx_models_from_phases(ctx, phases, ph->amplitudes->data, 0, 1);
+    free(phases);
+  } else if (flags & SpModelZeroPhases) {
     /* nb Fourier-space starts, transformed together on the device */
     float *all = (float *)malloc(sizeof(float) * 2 * n * (size_t)nb);
     for (int b = 0; b < nb; b++) {

@@ -229,6 +229,8 @@ struct spb_ctx {
   double *red = nullptr;       // reduce_scratch_doubles(nb)
   unsigned *nonfinite = nullptr;  // sticky flag of spb_ctx_nonfinite_async
   int *err_flag = nullptr;        // set by a kernel that gave up (bounded wait, misaligned TMA tile)
+  long long *hard = nullptr;      // random starts: elements the host evaluates (spb_ctx_models_from_phases)
+  unsigned *hard_n = nullptr;
   unsigned long long *seeds = nullptr;  // per-start generator keys (device starts)
   int x_valid = 0, xf_valid = 0;
   float xf_gamma1 = 0.0f;
@@ -633,7 +635,8 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   void *ptrs[] = {c->amp, c->amin, c->amax, c->pamp, c->flags, c->g[0], c->g[1], c->X, c->Y, c->Xf, c->Yf,
                   c->gp, c->T, c->absb, c->gtab, c->sel, c->red, c->nonfinite, c->err_flag, c->ax.tw, c->ay.tw,
                   c->az.tw,
-                  c->amp_line, c->amp_bad, c->meas_bits, c->beta_dev, c->beta_base, c->seeds, c->beta_zero, c->spar};
+                  c->amp_line, c->amp_bad, c->meas_bits, c->beta_dev, c->beta_base, c->seeds, c->beta_zero, c->spar,
+                  c->hard, c->hard_n};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : c->prof.ev) cudaEventDestroy(e);
@@ -920,6 +923,87 @@ static int models_from_fourier(spb_ctx *c, const float *fourier, int one, int re
 
 extern "C" int spb_ctx_model_from_fourier(spb_ctx *c, const float *fourier, int reset_others) {
   return models_from_fourier(c, fourier, 1, reset_others);
+}
+
+namespace spb {
+// Whether the float rounding of the double p could differ from that of a
+// double within 16 ulps of it: a rounding midpoint between two floats lies
+// that close (or p is too close to the ends of the float range to tell).
+__device__ __forceinline__ bool near_float_midpoint(double p) {
+  const double ap = fabs(p);
+  if (ap == 0.0) return false;
+  if (ap < 1e-30 || ap > 1e38) return true;
+  const float f = __double2float_rn(p);
+  const double up = 0.5 * ((double)f + (double)nextafterf(f, INFINITY));  // exact: two neighbouring floats
+  const double dn = 0.5 * ((double)f + (double)nextafterf(f, -INFINITY));
+  int e;
+  frexp(ap, &e);  // ap = m 2^e, m in [1/2, 1): one ulp is 2^(e-53)
+  return fmin(fabs(p - up), fabs(p - dn)) <= ldexp(16.0, e - 53);
+}
+
+// T[k] (k = b*n + i) = the random-phase start of pixel i from its phase, as
+// the reference's sp_image_rephase computes it (src/image_util.c:1035-1067):
+// (cos(phase) |amp|, sin(phase) |amp|) in double, rounded to float, |amp| as
+// sp_cabs of (amp, 0).  CUDA's double sincos is within 2 ulps of the exact
+// values and the C library's cos and sin within 1, so the two can round to
+// different floats only where a product lies within a few ulps of a float
+// rounding midpoint: such elements are listed in hard[] (up to cap) for the
+// host to evaluate with the C library.  phase holds one start (one) or nb.
+__global__ void phases_to_spectra_kernel(float2 *T, const float *amp, const float *phase, long long n, int nb, int one,
+                                         unsigned *hard_n, long long *hard, unsigned cap) {
+  const long long total = n * nb;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const long long i = k % n;
+    const float ph = phase[one ? i : k];
+    const float a = cabs_ref(make_float2(amp[i], 0.0f));
+    double sn, cs;
+    sincos((double)ph, &sn, &cs);
+    const double pr = cs * (double)a, pi = sn * (double)a;
+    T[k] = make_float2(__double2float_rn(pr), __double2float_rn(pi));
+    if (near_float_midpoint(pr) || near_float_midpoint(pi)) {
+      const unsigned slot = atomicAdd(hard_n, 1u);
+      if (slot < cap) hard[slot] = k;
+    }
+  }
+}
+}  // namespace spb
+
+// elements of a random start the host may have to evaluate (typically none)
+constexpr unsigned kHardCap = 4096;
+
+extern "C" int spb_ctx_models_from_phases(spb_ctx *c, const float *phases, const float *amp, int one,
+                                          int reset_others) {
+  const long long count = (long long)c->n * (one ? 1 : c->nb);
+  if (!c->hard) CK(cudaMalloc(&c->hard, sizeof(long long) * kHardCap));
+  if (!c->hard_n) CK(cudaMalloc(&c->hard_n, sizeof(unsigned)));
+  CK(cudaMemcpyAsync(c->absb, phases, sizeof(float) * (size_t)count, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemsetAsync(c->hard_n, 0, sizeof(unsigned), c->st));
+  phases_to_spectra_kernel<<<1184, 256, 0, c->st>>>(c->T, c->amp, c->absb, c->n, c->nb, one, c->hard_n, c->hard,
+                                                     kHardCap);
+  CK(cudaGetLastError());
+  c->launches++;
+  unsigned nh = 0;
+  CK(cudaMemcpyAsync(&nh, c->hard_n, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (nh > kHardCap) return fail("random start: %u elements near a float rounding midpoint (more than %u)", nh, kHardCap);
+  if (nh) {
+    std::vector<long long> ks(nh);
+    CK(cudaMemcpy(ks.data(), c->hard, sizeof(long long) * nh, cudaMemcpyDeviceToHost));
+    std::vector<float2> v(nh);
+    for (unsigned j = 0; j < nh; j++) {
+      const long long k = ks[j], i = k % c->n;
+      const float ph = phases[one ? i : k];
+      const float s2 = 0.0f * 0.0f + amp[i] * amp[i];  // sp_cabs of (amp, 0)
+      const float a = (float)sqrt((double)s2);
+      v[j] = make_float2((float)(cos((double)ph) * (double)a), (float)(sin((double)ph) * (double)a));
+    }
+    for (unsigned j = 0; j < nh; j++)
+      CK(cudaMemcpyAsync(c->T + ks[j], &v[j], sizeof(float2), cudaMemcpyHostToDevice, c->st));
+  }
+  if (inverse_scaled_into_model(c)) return -1;
+  if (reset_others && reset_iterates(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
 }
 
 extern "C" int spb_ctx_models_from_fourier(spb_ctx *c, const float *fourier, int reset_others) {
