@@ -10,4 +10,11 @@
  * (image.c; drawn on all host threads). */
 void spb_random_phases(float *phase, long long n);
 
+/* Runs fn(ctx, t, i0, i1) over [0, n) in contiguous spans on up to 8 host
+ * threads (one span when n is small); span t covers [i0, i1).  Returns the
+ * number of spans (at most SPB_PAR_MAX). */
+#define SPB_PAR_MAX 8
+typedef void (*spb_span_fn)(void *ctx, int t, long long i0, long long i1);
+int spb_parallel_for(long long n, spb_span_fn fn, void *ctx);
+
 #endif

@@ -350,6 +350,42 @@ void spb_random_phases(float *phase, long long n) {
   for (long long i = 0; i < n; i++) phase[i] = p_drand48() * 3.14159265358979323846 * 2;
 }
 
+typedef struct {
+  spb_span_fn fn;
+  void *ctx;
+  int t;
+  long long i0, i1;
+} par_span;
+
+static void *par_worker(void *arg) {
+  par_span *s = (par_span *)arg;
+  s->fn(s->ctx, s->t, s->i0, s->i1);
+  return NULL;
+}
+
+int spb_parallel_for(long long n, spb_span_fn fn, void *ctx) {
+  long long nt = n >= (1 << 18) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
+  if (nt > SPB_PAR_MAX) nt = SPB_PAR_MAX;
+  if (nt < 1) nt = 1;
+  pthread_t th[SPB_PAR_MAX];
+  par_span span[SPB_PAR_MAX];
+  int started[SPB_PAR_MAX] = {0};
+  for (long long t = 0; t < nt; t++) {
+    span[t].fn = fn;
+    span[t].ctx = ctx;
+    span[t].t = (int)t;
+    span[t].i0 = n * t / nt;
+    span[t].i1 = n * (t + 1) / nt;
+    if (t > 0) started[t] = pthread_create(&th[t], NULL, par_worker, &span[t]) == 0;
+  }
+  par_worker(&span[0]);
+  for (long long t = 1; t < nt; t++) {
+    if (started[t]) pthread_join(th[t], NULL);
+    else par_worker(&span[t]); /* no thread: run the span here */
+  }
+  return (int)nt;
+}
+
 void sp_image_rephase(Image *img, int type) {
   img->phased = 1;
   const long long n = sp_image_size(img);

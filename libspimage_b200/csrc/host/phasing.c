@@ -201,15 +201,28 @@ void sp_phaser_set_model(SpPhaser *ph, const Image *model) {
 }
 
 /* phasing.c:207-232 */
+/* the support bit of every pixel from a support image (on the host threads) */
+typedef struct {
+  SpPhaser *ph;
+  const Image *support;
+} support_job;
+
+static void support_span(void *ctx, int t, long long i0, long long i1) {
+  (void)t;
+  const support_job *j = (const support_job *)ctx;
+  for (long long i = i0; i < i1; i++) {
+    if (sp_real(j->support->image->data[i])) j->ph->pixel_flags->data[i] |= SpPixelInsideSupport;
+    else j->ph->pixel_flags->data[i] &= ~SpPixelInsideSupport;
+  }
+}
+
 void sp_phaser_set_support(SpPhaser *ph, const Image *support) {
   phaser_check_dimensions(ph, support);
   ph->support_iteration = -1;
   ensure_flags(ph);
   sync_flags_to_host(ph);
-  for (int i = 0; i < ph->image_size; i++) {
-    if (sp_real(support->image->data[i])) ph->pixel_flags->data[i] |= SpPixelInsideSupport;
-    else ph->pixel_flags->data[i] &= ~SpPixelInsideSupport;
-  }
+  support_job job = {ph, support};
+  spb_parallel_for(ph->image_size, support_span, &job);
   state(ph)->flags_dirty = 1;
 }
 
@@ -229,21 +242,37 @@ void sp_phaser_set_phased_amplitudes(SpPhaser *ph, const Image *pa) {
 }
 
 /* phasing.c:294-333 */
+/* amplitudes and measured bits from an amplitude image (on the host threads) */
+typedef struct {
+  SpPhaser *ph;
+  const Image *img;
+  long long masked[SPB_PAR_MAX];
+} set_amp_job;
+
+static void set_amp_span(void *ctx, int t, long long i0, long long i1) {
+  set_amp_job *j = (set_amp_job *)ctx;
+  long long masked = 0;
+  for (long long i = i0; i < i1; i++) {
+    j->ph->amplitudes->data[i] = sp_real(j->img->image->data[i]);
+    if (j->img->mask->data[i]) {
+      j->ph->pixel_flags->data[i] |= SpPixelMeasuredAmplitude;
+      masked++;
+    } else {
+      j->ph->pixel_flags->data[i] &= ~SpPixelMeasuredAmplitude;
+    }
+  }
+  j->masked[t] = masked;
+}
+
 void sp_phaser_set_amplitudes(SpPhaser *ph, const Image *amplitudes) {
   phaser_check_dimensions(ph, amplitudes);
   if (!ph->amplitudes) ph->amplitudes = sp_3matrix_alloc(ph->nx, ph->ny, ph->nz);
   ensure_flags(ph);
   sync_flags_to_host(ph);
-  int masked = 0;
-  for (int i = 0; i < ph->image_size; i++) {
-    ph->amplitudes->data[i] = sp_real(amplitudes->image->data[i]);
-    if (amplitudes->mask->data[i]) {
-      ph->pixel_flags->data[i] |= SpPixelMeasuredAmplitude;
-      masked++;
-    } else {
-      ph->pixel_flags->data[i] &= ~SpPixelMeasuredAmplitude;
-    }
-  }
+  set_amp_job job = {ph, amplitudes, {0}};
+  const int spans = spb_parallel_for(ph->image_size, set_amp_span, &job);
+  long long masked = 0;
+  for (int t = 0; t < spans; t++) masked += job.masked[t];
   if (masked == 0) fprintf(stderr, "Amplitudes mask is all zeros!\n");
   state(ph)->amp_dirty = 1;
   state(ph)->flags_dirty = 1;
@@ -648,10 +677,8 @@ int sp_phaser_init_support(SpPhaser *ph, const Image *support, int flags, real v
     phaser_check_dimensions(ph, support);
     ensure_flags(ph);
     sync_flags_to_host(ph);
-    for (int i = 0; i < ph->image_size; i++) {
-      if (sp_real(support->image->data[i])) ph->pixel_flags->data[i] |= SpPixelInsideSupport;
-      else ph->pixel_flags->data[i] &= ~SpPixelInsideSupport;
-    }
+    support_job job = {ph, support};
+    spb_parallel_for(ph->image_size, support_span, &job);
     state(ph)->flags_dirty = 1;
     ph->support_iteration = -1;
     return 0;
