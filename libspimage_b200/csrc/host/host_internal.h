@@ -10,6 +10,10 @@
  * (image.c; drawn on all host threads). */
 void spb_random_phases(float *phase, long long n);
 
+/* u[i] = p_drand48() for n consecutive draws, the same values and generator
+ * state as n calls (drawn on all host threads) */
+void spb_random_uniforms(float *u, long long n);
+
 /* Runs fn(ctx, t, i0, i1) over [0, n) in contiguous spans on up to 8 host
  * threads (one span when n is small); span t covers [i0, i1).  Returns the
  * number of spans (at most SPB_PAR_MAX). */

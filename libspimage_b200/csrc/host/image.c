@@ -302,13 +302,14 @@ static void rephase_parallel(Complex *data, const uint32_t *w, long long n) {
  * calls of rand() leave it -- the phases sp_image_rephase(SP_RANDOM_PHASE)
  * would use for an image of n pixels (drawn on all host threads). */
 typedef struct {
-  float *phase;
+  float *out;
   const uint32_t *w;
   long long i0, i1;
-} phase_span;
+  int phases; /* 1: p_drand48() * 2 pi rounded to float, 0: p_drand48() */
+} draw_span;
 
-static void *phase_worker(void *arg) {
-  const phase_span *s = (const phase_span *)arg;
+static void *draw_worker(void *arg) {
+  const draw_span *s = (const draw_span *)arg;
   uint32_t buf[RNG_DEG];
   rng_window_at(s->w, s->i0, buf);
   int f = 0, r = RNG_DEG - RNG_SEP;
@@ -318,37 +319,48 @@ static void *phase_worker(void *arg) {
     f = f + 1 == RNG_DEG ? 0 : f + 1;
     r = r + 1 == RNG_DEG ? 0 : r + 1;
     const real u = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
-    s->phase[i] = u * 3.14159265358979323846 * 2;
+    s->out[i] = s->phases ? (real)(u * 3.14159265358979323846 * 2) : u;
   }
   return NULL;
 }
 
-void spb_random_phases(float *phase, long long n) {
+/* n consecutive p_drand48() values (phases = 0) or phases (phases = 1) into
+ * out[], drawn on the host threads from the words n calls of rand() would
+ * return, the generator left where they leave it */
+static void draw_parallel(float *out, long long n, int phases) {
   uint32_t w[RNG_DEG];
   if (n > 0 && rng_take(n, w)) {
     long long nt = n >= (1 << 18) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
     if (nt < 1) nt = 1;
     if (nt > REPHASE_MAX_THREADS) nt = REPHASE_MAX_THREADS;
     pthread_t th[REPHASE_MAX_THREADS];
-    phase_span span[REPHASE_MAX_THREADS];
+    draw_span span[REPHASE_MAX_THREADS];
     int started[REPHASE_MAX_THREADS] = {0};
     for (long long t = 0; t < nt; t++) {
-      span[t].phase = phase;
+      span[t].out = out;
       span[t].w = w;
       span[t].i0 = n * t / nt;
       span[t].i1 = n * (t + 1) / nt;
-      if (t > 0) started[t] = pthread_create(&th[t], NULL, phase_worker, &span[t]) == 0;
+      span[t].phases = phases;
+      if (t > 0) started[t] = pthread_create(&th[t], NULL, draw_worker, &span[t]) == 0;
     }
-    phase_worker(&span[0]);
+    draw_worker(&span[0]);
     for (long long t = 1; t < nt; t++) {
       if (started[t]) pthread_join(th[t], NULL);
-      else phase_worker(&span[t]);
+      else draw_worker(&span[t]);
     }
     return;
   }
-  /* another generator layout: one rand() per pixel */
-  for (long long i = 0; i < n; i++) phase[i] = p_drand48() * 3.14159265358979323846 * 2;
+  /* another generator layout: one rand() per value */
+  for (long long i = 0; i < n; i++) {
+    const real u = p_drand48();
+    out[i] = phases ? (real)(u * 3.14159265358979323846 * 2) : u;
+  }
 }
+
+void spb_random_uniforms(float *u, long long n) { draw_parallel(u, n, 0); }
+
+void spb_random_phases(float *phase, long long n) { draw_parallel(phase, n, 1); }
 
 typedef struct {
   spb_span_fn fn;

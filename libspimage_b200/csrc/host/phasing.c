@@ -485,12 +485,24 @@ static int draw_start(SpPhaser *ph, int flags, Image *m) {
   double sum = 0;
   for (int i = 0; i < n; i++) sum += ph->amplitudes->data[i] * ph->amplitudes->data[i];
   sum /= n;
-  for (int i = 0; i < n; i++) {
-    /* the reference's sp_cinit(p_drand48()-0.5, p_drand48()-0.5) draws the
-     * imaginary part first under gcc's argument evaluation order */
-    const real im = p_drand48() - 0.5;
-    const real re = p_drand48() - 0.5;
-    m->image->data[i] = sp_cinit(re, im);
+  /* the reference's sp_cinit(p_drand48()-0.5, p_drand48()-0.5) draws the
+   * imaginary part first under gcc's argument evaluation order: pixel i takes
+   * draws 2i (imaginary) and 2i + 1 (real) */
+  float *u = (float *)malloc(sizeof(float) * 2 * (size_t)n);
+  if (u) {
+    spb_random_uniforms(u, 2 * (long long)n);
+    for (int i = 0; i < n; i++) {
+      const real im = u[2 * (size_t)i] - 0.5;
+      const real re = u[2 * (size_t)i + 1] - 0.5;
+      m->image->data[i] = sp_cinit(re, im);
+    }
+    free(u);
+  } else {
+    for (int i = 0; i < n; i++) {
+      const real im = p_drand48() - 0.5;
+      const real re = p_drand48() - 0.5;
+      m->image->data[i] = sp_cinit(re, im);
+    }
   }
   double msum = 0;
   for (int i = 0; i < n; i++) msum += sp_cabs2(m->image->data[i]);

@@ -100,3 +100,24 @@ def test_concurrent_rephase_keeps_the_generator(env):
     assert not errors
     so.sp_srand(123)
     assert [libc.rand() for _ in range(64)] == want
+
+
+@pytest.mark.parametrize("n,seed,skip", [(5, 1, 0), (40, 3, 7), (600000, 8, 2)])
+def test_uniform_draw_matches_rand(env, n, seed, skip):
+    """The p_drand48() values of a random-values start (two per pixel), drawn
+    on the host threads by jumping ahead in the generator, equal n calls of
+    rand() / RAND_MAX, and rand() continues where those calls leave it."""
+    L, so, libc, libm = env
+    so.spb_random_uniforms.argtypes = [C.c_void_p, C.c_longlong]
+    libc.srand(seed)
+    for _ in range(skip):
+        libc.rand()
+    got = np.empty(n, np.float32)
+    so.spb_random_uniforms(got.ctypes.data, n)
+    after = libc.rand()
+    libc.srand(seed)
+    for _ in range(skip):
+        libc.rand()
+    want = np.array([np.float32(float(libc.rand()) / RAND_MAX) for _ in range(n)], np.float32)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert after == libc.rand()
