@@ -1392,15 +1392,16 @@ static long long area_rank(long long n, float area) {
 }
 
 // dev: when set, the rank (area rule) or the relative threshold is read from
-// it at run time (captured support updates)
+// it at run time (captured support updates).  pdl: launch with programmatic
+// dependent launch (context streams with it enabled).
 static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *absv, long long n, int nb, int type,
-                              float value, uint8_t *flags, const SupportParams *dev = nullptr) {
+                              float value, uint8_t *flags, const SupportParams *dev = nullptr, bool pdl = false) {
   if (type == SPB_SUPPORT_AREA) {
-    CK(launch_select_kth_desc(absv, n, nb, area_rank(n, value), sel, st, dev ? &dev->rank : nullptr));
-    CK(launch_mask_from_abs(absv, sel, 0.0f, 0, flags, n, nb, st));
+    CK(launch_select_kth_desc(absv, n, nb, area_rank(n, value), sel, st, dev ? &dev->rank : nullptr, pdl));
+    CK(launch_mask_from_abs(absv, sel, 0.0f, 0, flags, n, nb, st, nullptr, pdl));
   } else if (type == SPB_SUPPORT_THRESHOLD) {
-    CK(launch_max_abs(absv, n, nb, sel, st));
-    CK(launch_mask_from_abs(absv, sel, value, 1, flags, n, nb, st, dev ? &dev->rel : nullptr));
+    CK(launch_max_abs(absv, n, nb, sel, st, pdl));
+    CK(launch_mask_from_abs(absv, sel, value, 1, flags, n, nb, st, dev ? &dev->rel : nullptr, pdl));
   } else {
     return fail("unknown support update type %d", type);
   }
@@ -1410,7 +1411,7 @@ static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *ab
 static int select_and_mask(spb_ctx *c, const float *absv, long long n, int nb, int type, float value,
                            uint8_t *flags, const SupportParams *dev = nullptr) {
   if (prof_begin(c)) return -1;
-  if (select_and_mask_on(c->st, c->sel, absv, n, nb, type, value, flags, dev)) return -1;
+  if (select_and_mask_on(c->st, c->sel, absv, n, nb, type, value, flags, dev, c->tune[SPB_TUNE_NO_PDL] == 0)) return -1;
   c->launches += (type == SPB_SUPPORT_AREA) ? 6 : 4;  // init, four histogram passes, mask | init, max, finish, mask
   return prof_end(c, type == SPB_SUPPORT_AREA ? 16 : 17);
 }

@@ -152,11 +152,13 @@ cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArg
 // support selection and reductions; nb starts of n pixels each, start b at offset b*n
 // k_dev / rel_dev: when set, the rank k / the relative threshold is read from
 // device memory at run time instead of the value argument
+// pdl: launch with programmatic dependent launch (each kernel waits for its
+// predecessor's grid before touching memory)
 cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long long k, SelectState *state,
-                                   cudaStream_t st, const unsigned long long *k_dev = nullptr);
-cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st);
+                                   cudaStream_t st, const unsigned long long *k_dev, bool pdl);
+cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st, bool pdl);
 cudaError_t launch_mask_from_abs(const float *absv, SelectState *state, float rel, int use_rel, uint8_t *flags,
-                                 long long n, int nb, cudaStream_t st, const float *rel_dev = nullptr);
+                                 long long n, int nb, cudaStream_t st, const float *rel_dev, bool pdl);
 // out[b*4 + k]; scratch of reduce_scratch_doubles(nb) doubles starting at out
 int reduce_scratch_doubles(int nb);
 cudaError_t launch_reduce_efourier(const float2 *F, const float *amp, const uint8_t *flags, long long n, int nb,

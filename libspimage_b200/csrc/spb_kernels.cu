@@ -12,6 +12,7 @@
 #include <math.h>
 
 #include "spb_internal.h"
+#include "spb_passes.cuh"
 #include "spb_pointwise.cuh"
 
 namespace spb {
@@ -449,6 +450,8 @@ cudaError_t launch_col(int mode, const LinePlan &pl, int line_len, const PassArg
 // up instead of evaluating it per pixel, and every start of a batch shares
 // the table.  Same function, same floats.
 __global__ void gauss_table_kernel(PassArgs a, float *__restrict__ tab) {
+  pdl_wait();
+  pdl_release();  // the table is read by the blur pass, which waits for this grid
   const int hx = a.nx / 2 + 1, hy = a.ny / 2 + 1;
   const long long total = (long long)hx * hy * (a.nz / 2 + 1);
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -461,8 +464,7 @@ cudaError_t launch_gauss_table(const PassArgs &a, float *tab, cudaStream_t st) {
   const long long total = (long long)(a.nx / 2 + 1) * (a.ny / 2 + 1) * (a.nz / 2 + 1);
   long long blocks = (total + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
-  gauss_table_kernel<<<(unsigned)blocks, 256, 0, st>>>(a, tab);
-  return cudaGetLastError();
+  return launch_maybe_pdl(gauss_table_kernel, dim3((unsigned)blocks), dim3(256), 0, st, a.pdl != 0, a, tab);
 }
 
 // ------------------------------------------------- support selection kernels
@@ -530,6 +532,7 @@ __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restric
   v += (long long)b * n;
   s += b;
   for (int i = threadIdx.x; i < 8 * SEL_BINS; i += blockDim.x) (&h[0][0])[i] = 0;
+  pdl_wait();
   if (pass == 0) {
     if (threadIdx.x == 0) {
       pm[0] = s->pass_prefix[0];
@@ -570,6 +573,7 @@ __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restric
     }
   }
   __syncthreads();
+  pdl_release();
   for (int d = threadIdx.x; d < SEL_BINS; d += blockDim.x) {
     unsigned int c = 0;
     for (int w = 0; w < 8; w++) c += h[w][d];
@@ -578,6 +582,8 @@ __global__ void __launch_bounds__(256) select_hist_kernel(const float *__restric
 }
 
 __global__ void select_init_kernel(SelectState *states, unsigned long long rank, const unsigned long long *rank_dev) {
+  pdl_wait();
+  pdl_release();
   SelectState *s = states + blockIdx.x;
   for (int d = threadIdx.x; d < 4 * SEL_BINS; d += blockDim.x) (&s->hist[0][0])[d] = 0;
   if (threadIdx.x == 0) {
@@ -599,14 +605,17 @@ static unsigned blocks_per_start(long long n, int nb) {
 
 // the four histogram passes; the last pick happens in the mask kernel
 cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long long k, SelectState *state,
-                                   cudaStream_t st, const unsigned long long *k_dev) {
-  select_init_kernel<<<nb, 256, 0, st>>>(state, (unsigned long long)k, k_dev);
+                                   cudaStream_t st, const unsigned long long *k_dev, bool pdl) {
+  cudaError_t e = launch_maybe_pdl(select_init_kernel, dim3(nb), dim3(256), 0, st, pdl, state, (unsigned long long)k, k_dev);
   const dim3 grid(blocks_per_start(n, nb), nb);
-  for (int p = 0; p < 4; p++) select_hist_kernel<<<grid, 256, 0, st>>>(absv, n, state, p);
-  return cudaGetLastError();
+  for (int p = 0; p < 4 && e == cudaSuccess; p++)
+    e = launch_maybe_pdl(select_hist_kernel, grid, dim3(256), 0, st, pdl, absv, n, state, p);
+  return e;
 }
 
 __global__ void max_abs_kernel(const float *__restrict__ v, long long n, SelectState *states) {
+  pdl_wait();
+  pdl_release();
   SelectState *s = states + blockIdx.y;
   v += (long long)blockIdx.y * n;
   unsigned int m = 0;
@@ -619,15 +628,19 @@ __global__ void max_abs_kernel(const float *__restrict__ v, long long n, SelectS
 }
 
 __global__ void max_finish_kernel(SelectState *states) {
+  pdl_wait();
+  pdl_release();
   SelectState *s = states + blockIdx.x;
   s->result = __uint_as_float(s->maxbits);
 }
 
-cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st) {
-  select_init_kernel<<<nb, 256, 0, st>>>(state, 0, nullptr);
-  max_abs_kernel<<<dim3(blocks_per_start(n, nb), nb), 256, 0, st>>>(absv, n, state);
-  max_finish_kernel<<<nb, 1, 0, st>>>(state);
-  return cudaGetLastError();
+cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st, bool pdl) {
+  cudaError_t e = launch_maybe_pdl(select_init_kernel, dim3(nb), dim3(256), 0, st, pdl, state, 0ULL,
+                                   (const unsigned long long *)nullptr);
+  if (e == cudaSuccess)
+    e = launch_maybe_pdl(max_abs_kernel, dim3(blocks_per_start(n, nb), nb), dim3(256), 0, st, pdl, absv, n, state);
+  if (e == cudaSuccess) e = launch_maybe_pdl(max_finish_kernel, dim3(nb), dim3(1), 0, st, pdl, state);
+  return e;
 }
 
 // support_from_absolute_threshold (src/support_update.c:392-400): strict '>'.
@@ -639,6 +652,7 @@ __global__ void mask_kernel(const float *__restrict__ v, SelectState *states, fl
   __shared__ unsigned long long pr;
   const int b = blockIdx.y;
   SelectState *s = states + b;
+  pdl_wait();
   float t;
   if (use_rel) {
     t = __fmul_rn(s->result, rel_dev ? *rel_dev : rel);
@@ -651,6 +665,7 @@ __global__ void mask_kernel(const float *__restrict__ v, SelectState *states, fl
     __syncthreads();
     t = __uint_as_float(pm[0]);
   }
+  pdl_release();
   v += (long long)b * n;
   flags += (long long)b * n;
   // four elements per thread and round, their loads in flight together
@@ -673,9 +688,9 @@ __global__ void mask_kernel(const float *__restrict__ v, SelectState *states, fl
 }
 
 cudaError_t launch_mask_from_abs(const float *absv, SelectState *state, float rel, int use_rel, uint8_t *flags,
-                                 long long n, int nb, cudaStream_t st, const float *rel_dev) {
-  mask_kernel<<<dim3(blocks_per_start(n, nb), nb), 256, 0, st>>>(absv, state, rel, use_rel, flags, n, rel_dev);
-  return cudaGetLastError();
+                                 long long n, int nb, cudaStream_t st, const float *rel_dev, bool pdl) {
+  return launch_maybe_pdl(mask_kernel, dim3(blocks_per_start(n, nb), nb), dim3(256), 0, st, pdl, absv, state, rel,
+                          use_rel, flags, n, rel_dev);
 }
 
 // ---------------------------------------------------------------- reductions
