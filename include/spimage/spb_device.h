@@ -214,6 +214,16 @@ int spb_ctx_models_from_fourier(spb_ctx *ctx, const float *fourier, int reset_ot
  * a float rounding midpoint) are evaluated on the host with the C library,
  * so the result is the reference's bit for bit. */
 int spb_ctx_models_from_phases(spb_ctx *ctx, const float *phases, const float *amp, int one, int reset_others);
+/* A page-locked host buffer of at least `bytes` owned by the context (no
+ * reference counterpart): the host API draws random phases and converts pixel
+ * flags into it, so their uploads run by DMA.  Valid until the next call
+ * asks for more bytes or the context is destroyed; NULL on failure. */
+void *spb_ctx_host_stage(spb_ctx *ctx, size_t bytes);
+/* Page-lock (0 on success) / release a host range the caller keeps and
+ * reuses across calls, so copies to and from it run by DMA (the host API
+ * locks its amplitude array and its model image). */
+int spb_host_register(void *p, size_t bytes);
+void spb_host_unregister(void *p);
 /* g1[b] = IFFT(amp * exp(2 pi i u))/N with u drawn on the device by
  * Philox4x32-10 keyed by seeds[b] (throughput runs; the host API's
  * SpModelRandomPhases reproduces the reference's rand() stream instead) */

@@ -244,123 +244,62 @@ static int rng_take(long long n, uint32_t *w) {
 #endif
 }
 
-/* Random-phase rephasing of pixels [i0, i1): the words of draws i0.. come
- * from the window w of the 31 words before draw 0; each pixel's phase is
- * p_drand48() * 2 pi rounded to float and its value
- * (cos(phase) * |v|, sin(phase) * |v|) is evaluated with the same double libm
- * calls and roundings as the reference's loop -- on whichever thread, the
- * same bits. */
-typedef struct {
-  Complex *data;
-  const uint32_t *w;
-  long long i0, i1;
-} rephase_span;
+/* ------------------------------------------------------------ host threads
+ * Worker threads started on first use and kept for the process: a parallel
+ * loop wakes them instead of creating threads per call (creating and joining
+ * fifteen threads cost about 0.3 ms a call, several times per start).  One
+ * loop at a time runs on the pool; a caller that finds it taken by another
+ * host thread runs its spans on threads of its own.  The spans, and so the
+ * results, are the same either way.  A child forked while the pool exists
+ * starts with an empty one. */
+#define SPB_POOL_MAX 32
 
-static void *rephase_worker(void *arg) {
-  const rephase_span *s = (const rephase_span *)arg;
-  uint32_t buf[RNG_DEG];
-  rng_window_at(s->w, s->i0, buf); /* the 31 words before draw i0 */
-  int f = 0, r = RNG_DEG - RNG_SEP;
-  for (long long i = s->i0; i < s->i1; i++) {
-    const uint32_t val = buf[f] + buf[r];
-    buf[f] = val;
-    f = f + 1 == RNG_DEG ? 0 : f + 1;
-    r = r + 1 == RNG_DEG ? 0 : r + 1;
-    const real u = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
-    const real phase = u * 3.14159265358979323846 * 2;
-    const real amp = sp_cabs(s->data[i]);
-    s->data[i].re = cos(phase) * amp;
-    s->data[i].im = sin(phase) * amp;
+static struct {
+  pthread_mutex_t run; /* held by the caller whose loop is on the pool */
+  pthread_mutex_t mu;
+  pthread_cond_t go, done;
+  int workers;                        /* started: ids 1..workers */
+  unsigned long gen;                  /* loops posted */
+  unsigned long born[SPB_POOL_MAX];   /* gen when worker id was started */
+  int pending;                        /* workers still in the current loop */
+  int nt;
+  long long n;
+  spb_span_fn fn;
+  void *ctx;
+} pool = {PTHREAD_MUTEX_INITIALIZER, PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER,
+          PTHREAD_COND_INITIALIZER, 0, 0, {0}, 0, 0, 0, NULL, NULL};
+
+static void pool_after_fork_child(void) {
+  pthread_mutex_init(&pool.run, NULL);
+  pthread_mutex_init(&pool.mu, NULL);
+  pthread_cond_init(&pool.go, NULL);
+  pthread_cond_init(&pool.done, NULL);
+  pool.workers = 0;
+  pool.pending = 0;
+}
+
+static pthread_once_t pool_once = PTHREAD_ONCE_INIT;
+static void pool_register_fork(void) { pthread_atfork(NULL, NULL, pool_after_fork_child); }
+
+static void *pool_main(void *arg) {
+  const int id = (int)(intptr_t)arg;
+  pthread_mutex_lock(&pool.mu);
+  unsigned long seen = pool.born[id];
+  for (;;) {
+    while (pool.gen == seen) pthread_cond_wait(&pool.go, &pool.mu);
+    seen = pool.gen;
+    if (id < pool.nt) {
+      const spb_span_fn fn = pool.fn;
+      void *ctx = pool.ctx;
+      const long long n = pool.n, nt = pool.nt;
+      pthread_mutex_unlock(&pool.mu);
+      fn(ctx, id, n * id / nt, n * (id + 1) / nt);
+      pthread_mutex_lock(&pool.mu);
+      if (--pool.pending == 0) pthread_cond_signal(&pool.done);
+    }
   }
   return NULL;
 }
-
-#define REPHASE_MAX_THREADS 32
-static void rephase_parallel(Complex *data, const uint32_t *w, long long n) {
-  long long nt = n >= (1 << 16) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
-  if (nt < 1) nt = 1;
-  if (nt > REPHASE_MAX_THREADS) nt = REPHASE_MAX_THREADS;
-  pthread_t th[REPHASE_MAX_THREADS];
-  rephase_span span[REPHASE_MAX_THREADS];
-  int started[REPHASE_MAX_THREADS] = {0};
-  for (long long t = 0; t < nt; t++) {
-    span[t].data = data;
-    span[t].w = w;
-    span[t].i0 = n * t / nt;
-    span[t].i1 = n * (t + 1) / nt;
-    if (t > 0) started[t] = pthread_create(&th[t], NULL, rephase_worker, &span[t]) == 0;
-  }
-  rephase_worker(&span[0]);
-  for (long long t = 1; t < nt; t++) {
-    if (started[t]) pthread_join(th[t], NULL);
-    else rephase_worker(&span[t]); /* no thread: do the span here */
-  }
-}
-
-/* The phases alone: phase[i] = p_drand48() * 2 pi rounded to float, from the
- * same rand() words, in the same pixel order, leaving the generator where n
- * calls of rand() leave it -- the phases sp_image_rephase(SP_RANDOM_PHASE)
- * would use for an image of n pixels (drawn on all host threads). */
-typedef struct {
-  float *out;
-  const uint32_t *w;
-  long long i0, i1;
-  int phases; /* 1: p_drand48() * 2 pi rounded to float, 0: p_drand48() */
-} draw_span;
-
-static void *draw_worker(void *arg) {
-  const draw_span *s = (const draw_span *)arg;
-  uint32_t buf[RNG_DEG];
-  rng_window_at(s->w, s->i0, buf);
-  int f = 0, r = RNG_DEG - RNG_SEP;
-  for (long long i = s->i0; i < s->i1; i++) {
-    const uint32_t val = buf[f] + buf[r];
-    buf[f] = val;
-    f = f + 1 == RNG_DEG ? 0 : f + 1;
-    r = r + 1 == RNG_DEG ? 0 : r + 1;
-    const real u = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
-    s->out[i] = s->phases ? (real)(u * 3.14159265358979323846 * 2) : u;
-  }
-  return NULL;
-}
-
-/* n consecutive p_drand48() values (phases = 0) or phases (phases = 1) into
- * out[], drawn on the host threads from the words n calls of rand() would
- * return, the generator left where they leave it */
-static void draw_parallel(float *out, long long n, int phases) {
-  uint32_t w[RNG_DEG];
-  if (n > 0 && rng_take(n, w)) {
-    long long nt = n >= (1 << 18) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
-    if (nt < 1) nt = 1;
-    if (nt > REPHASE_MAX_THREADS) nt = REPHASE_MAX_THREADS;
-    pthread_t th[REPHASE_MAX_THREADS];
-    draw_span span[REPHASE_MAX_THREADS];
-    int started[REPHASE_MAX_THREADS] = {0};
-    for (long long t = 0; t < nt; t++) {
-      span[t].out = out;
-      span[t].w = w;
-      span[t].i0 = n * t / nt;
-      span[t].i1 = n * (t + 1) / nt;
-      span[t].phases = phases;
-      if (t > 0) started[t] = pthread_create(&th[t], NULL, draw_worker, &span[t]) == 0;
-    }
-    draw_worker(&span[0]);
-    for (long long t = 1; t < nt; t++) {
-      if (started[t]) pthread_join(th[t], NULL);
-      else draw_worker(&span[t]);
-    }
-    return;
-  }
-  /* another generator layout: one rand() per value */
-  for (long long i = 0; i < n; i++) {
-    const real u = p_drand48();
-    out[i] = phases ? (real)(u * 3.14159265358979323846 * 2) : u;
-  }
-}
-
-void spb_random_uniforms(float *u, long long n) { draw_parallel(u, n, 0); }
-
-void spb_random_phases(float *phase, long long n) { draw_parallel(phase, n, 1); }
 
 typedef struct {
   spb_span_fn fn;
@@ -375,28 +314,149 @@ static void *par_worker(void *arg) {
   return NULL;
 }
 
-int spb_parallel_for(long long n, spb_span_fn fn, void *ctx) {
-  long long nt = n >= (1 << 18) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
-  if (nt > SPB_PAR_MAX) nt = SPB_PAR_MAX;
-  if (nt < 1) nt = 1;
-  pthread_t th[SPB_PAR_MAX];
-  par_span span[SPB_PAR_MAX];
-  int started[SPB_PAR_MAX] = {0};
-  for (long long t = 0; t < nt; t++) {
+/* fn(ctx, t, i0, i1) for the nt contiguous spans of [0, n) */
+static void run_spans(int nt, long long n, spb_span_fn fn, void *ctx) {
+  if (nt <= 1) {
+    fn(ctx, 0, 0, n);
+    return;
+  }
+  if (nt > SPB_POOL_MAX) nt = SPB_POOL_MAX;
+  if (pthread_mutex_trylock(&pool.run) == 0) {
+    pthread_once(&pool_once, pool_register_fork);
+    pthread_mutex_lock(&pool.mu);
+    while (pool.workers < nt - 1) {
+      pthread_t th;
+      const int id = pool.workers + 1;
+      pool.born[id] = pool.gen;
+      if (pthread_create(&th, NULL, pool_main, (void *)(intptr_t)id) != 0) break;
+      pthread_detach(th);
+      pool.workers = id;
+    }
+    const int helpers = pool.workers < nt - 1 ? pool.workers : nt - 1;
+    pool.nt = nt;
+    pool.n = n;
+    pool.fn = fn;
+    pool.ctx = ctx;
+    pool.pending = helpers;
+    pool.gen++;
+    pthread_cond_broadcast(&pool.go);
+    pthread_mutex_unlock(&pool.mu);
+    fn(ctx, 0, 0, n / nt);
+    for (int t = helpers + 1; t < nt; t++) fn(ctx, t, n * t / nt, n * (t + 1) / nt); /* spans without a worker */
+    pthread_mutex_lock(&pool.mu);
+    while (pool.pending) pthread_cond_wait(&pool.done, &pool.mu);
+    pthread_mutex_unlock(&pool.mu);
+    pthread_mutex_unlock(&pool.run);
+    return;
+  }
+  /* the pool is busy with another caller's loop */
+  pthread_t th[SPB_POOL_MAX];
+  par_span span[SPB_POOL_MAX];
+  int started[SPB_POOL_MAX] = {0};
+  for (int t = 0; t < nt; t++) {
     span[t].fn = fn;
     span[t].ctx = ctx;
-    span[t].t = (int)t;
+    span[t].t = t;
     span[t].i0 = n * t / nt;
     span[t].i1 = n * (t + 1) / nt;
     if (t > 0) started[t] = pthread_create(&th[t], NULL, par_worker, &span[t]) == 0;
   }
   par_worker(&span[0]);
-  for (long long t = 1; t < nt; t++) {
+  for (int t = 1; t < nt; t++) {
     if (started[t]) pthread_join(th[t], NULL);
     else par_worker(&span[t]); /* no thread: run the span here */
   }
+}
+
+static int host_threads(long long n, long long min_n, int cap) {
+  long long nt = n >= min_n ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
+  if (nt > cap) nt = cap;
+  if (nt < 1) nt = 1;
   return (int)nt;
 }
+
+int spb_parallel_for(long long n, spb_span_fn fn, void *ctx) {
+  const int nt = host_threads(n, 1 << 18, SPB_PAR_MAX);
+  run_spans(nt, n, fn, ctx);
+  return nt;
+}
+
+/* Random-phase rephasing of pixels [i0, i1): the words of draws i0.. come
+ * from the window w of the 31 words before draw 0; each pixel's phase is
+ * p_drand48() * 2 pi rounded to float and its value
+ * (cos(phase) * |v|, sin(phase) * |v|) is evaluated with the same double libm
+ * calls and roundings as the reference's loop -- on whichever thread, the
+ * same bits. */
+typedef struct {
+  Complex *data;
+  const uint32_t *w;
+} rephase_job;
+
+static void rephase_span(void *arg, int t, long long i0, long long i1) {
+  (void)t;
+  const rephase_job *s = (const rephase_job *)arg;
+  uint32_t buf[RNG_DEG];
+  rng_window_at(s->w, i0, buf); /* the 31 words before draw i0 */
+  int f = 0, r = RNG_DEG - RNG_SEP;
+  for (long long i = i0; i < i1; i++) {
+    const uint32_t val = buf[f] + buf[r];
+    buf[f] = val;
+    f = f + 1 == RNG_DEG ? 0 : f + 1;
+    r = r + 1 == RNG_DEG ? 0 : r + 1;
+    const real u = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
+    const real phase = u * 3.14159265358979323846 * 2;
+    const real amp = sp_cabs(s->data[i]);
+    s->data[i].re = cos(phase) * amp;
+    s->data[i].im = sin(phase) * amp;
+  }
+}
+
+/* The phases alone: phase[i] = p_drand48() * 2 pi rounded to float, from the
+ * same rand() words, in the same pixel order, leaving the generator where n
+ * calls of rand() leave it -- the phases sp_image_rephase(SP_RANDOM_PHASE)
+ * would use for an image of n pixels (drawn on all host threads). */
+typedef struct {
+  float *out;
+  const uint32_t *w;
+  int phases; /* 1: p_drand48() * 2 pi rounded to float, 0: p_drand48() */
+} draw_job;
+
+static void draw_span(void *arg, int t, long long i0, long long i1) {
+  (void)t;
+  const draw_job *s = (const draw_job *)arg;
+  uint32_t buf[RNG_DEG];
+  rng_window_at(s->w, i0, buf);
+  int f = 0, r = RNG_DEG - RNG_SEP;
+  for (long long i = i0; i < i1; i++) {
+    const uint32_t val = buf[f] + buf[r];
+    buf[f] = val;
+    f = f + 1 == RNG_DEG ? 0 : f + 1;
+    r = r + 1 == RNG_DEG ? 0 : r + 1;
+    const real u = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
+    s->out[i] = s->phases ? (real)(u * 3.14159265358979323846 * 2) : u;
+  }
+}
+
+/* n consecutive p_drand48() values (phases = 0) or phases (phases = 1) into
+ * out[], drawn on the host threads from the words n calls of rand() would
+ * return, the generator left where they leave it */
+static void draw_parallel(float *out, long long n, int phases) {
+  uint32_t w[RNG_DEG];
+  if (n > 0 && rng_take(n, w)) {
+    draw_job job = {out, w, phases};
+    run_spans(host_threads(n, 1 << 18, SPB_POOL_MAX), n, draw_span, &job);
+    return;
+  }
+  /* another generator layout: one rand() per value */
+  for (long long i = 0; i < n; i++) {
+    const real u = p_drand48();
+    out[i] = phases ? (real)(u * 3.14159265358979323846 * 2) : u;
+  }
+}
+
+void spb_random_uniforms(float *u, long long n) { draw_parallel(u, n, 0); }
+
+void spb_random_phases(float *phase, long long n) { draw_parallel(phase, n, 1); }
 
 void sp_image_rephase(Image *img, int type) {
   img->phased = 1;
@@ -406,7 +466,8 @@ void sp_image_rephase(Image *img, int type) {
   } else if (type == SP_RANDOM_PHASE) {
     uint32_t w[RNG_DEG];
     if (n > 0 && rng_take(n, w)) {
-      rephase_parallel(img->image->data, w, n);
+      rephase_job job = {img->image->data, w};
+      run_spans(host_threads(n, 1 << 16, SPB_POOL_MAX), n, rephase_span, &job);
       return;
     }
     /* another generator layout: one rand() per pixel, as the reference */

@@ -22,6 +22,9 @@ typedef struct {
   int starts; /* independent reconstructions in the context (0 = 1) */
   int amp_dirty, flags_dirty, margins_dirty, pamp_dirty;
   int flags_dev_newer; /* device flags changed by a support update */
+  void *pinned_amp;    /* ph->amplitudes->data when page-locked */
+  void *pinned_model;  /* ph->model->image->data when page-locked */
+  Image *spare_model, *spare_change; /* the previous start's images while a new start is made */
 } dev_state;
 
 static char g_last_err[512];
@@ -37,6 +40,40 @@ static int dev_error(const char *where) {
 static dev_state *state(SpPhaser *ph) {
   if (!ph->device) ph->device = calloc(1, sizeof(dev_state));
   return (dev_state *)ph->device;
+}
+
+/* A new start takes the model and model-change images off the phaser (the
+ * phaser has no model until the start succeeds, as in the reference, which
+ * frees them) and keeps them to reuse: a fresh 1024^2 image costs page faults
+ * on its first download every start. */
+static void release_model_images(SpPhaser *ph) {
+  dev_state *s = state(ph);
+  if (ph->model) {
+    if (s->spare_model) sp_image_free(s->spare_model);
+    s->spare_model = ph->model;
+    ph->model = NULL;
+  }
+  if (ph->model_change) {
+    if (s->spare_change) sp_image_free(s->spare_change);
+    s->spare_change = ph->model_change;
+    ph->model_change = NULL;
+  }
+}
+
+static void free_spare_model_images(SpPhaser *ph) {
+  dev_state *s = state(ph);
+  if (s->spare_model) {
+    if (s->pinned_model == s->spare_model->image->data) {
+      spb_host_unregister(s->pinned_model);
+      s->pinned_model = NULL;
+    }
+    sp_image_free(s->spare_model);
+    s->spare_model = NULL;
+  }
+  if (s->spare_change) {
+    sp_image_free(s->spare_change);
+    s->spare_change = NULL;
+  }
 }
 
 static int ensure_ctx(SpPhaser *ph) {
@@ -156,6 +193,13 @@ void sp_phaser_set_objective(SpPhaser *ph, SpPhasingObjective obj) { ph->phasing
 
 void sp_phaser_free(SpPhaser *ph) {
   if (!ph) return;
+  if (ph->device) {
+    dev_state *s = (dev_state *)ph->device;
+    free_spare_model_images(ph);
+    spb_host_unregister(s->pinned_model);
+    spb_host_unregister(s->pinned_amp);
+    s->pinned_model = s->pinned_amp = NULL;
+  }
   Image **imgs[] = {&ph->model, &ph->model_before_projection, &ph->model_change, &ph->amplitudes_image,
                     &ph->old_model, &ph->support, &ph->fmodel};
   for (size_t i = 0; i < sizeof(imgs) / sizeof(imgs[0]); i++)
@@ -266,7 +310,11 @@ static void set_amp_span(void *ctx, int t, long long i0, long long i1) {
 
 void sp_phaser_set_amplitudes(SpPhaser *ph, const Image *amplitudes) {
   phaser_check_dimensions(ph, amplitudes);
-  if (!ph->amplitudes) ph->amplitudes = sp_3matrix_alloc(ph->nx, ph->ny, ph->nz);
+  if (!ph->amplitudes) {
+    ph->amplitudes = sp_3matrix_alloc(ph->nx, ph->ny, ph->nz);
+    if (!spb_host_register(ph->amplitudes->data, sizeof(real) * (size_t)ph->image_size))
+      state(ph)->pinned_amp = ph->amplitudes->data;
+  }
   ensure_flags(ph);
   sync_flags_to_host(ph);
   set_amp_job job = {ph, amplitudes, {0}};
@@ -441,8 +489,7 @@ int sp_phaser_init_model(SpPhaser *ph, const Image *user_model, int flags) {
     snprintf(g_last_err, sizeof(g_last_err), "sp_phaser_init must succeed before sp_phaser_init_model");
     return -3;
   }
-  if (ph->model) { sp_image_free(ph->model); ph->model = NULL; }
-  if (ph->model_change) { sp_image_free(ph->model_change); ph->model_change = NULL; }
+  release_model_images(ph);
   if (!user_model && !(flags & (SpModelRandomPhases | SpModelZeroPhases | SpModelRandomValues))) return -3;
   if (user_model) phaser_check_dimensions(ph, user_model);
   if (sync_to_device(ph)) return -8;
@@ -456,11 +503,10 @@ int sp_phaser_init_model(SpPhaser *ph, const Image *user_model, int flags) {
       snprintf(g_last_err, sizeof(g_last_err), "sp_phaser_init_model: set the amplitudes before a random-phase start");
       return -3;
     }
-    float *phases = (float *)malloc(sizeof(float) * (size_t)ph->image_size);
-    if (!phases) return -8;
+    float *phases = (float *)spb_ctx_host_stage(ctx, sizeof(float) * (size_t)ph->image_size);
+    if (!phases) return dev_error("init model");
     spb_random_phases(phases, ph->image_size);
     rc = spb_ctx_models_from_phases(ctx, phases, ph->amplitudes->data, 1, 1);
-    free(phases);
   } else {
     Image *m = sp_image_alloc(ph->nx, ph->ny, ph->nz);
     if (draw_start(ph, flags, m)) rc = spb_ctx_model_from_fourier(ctx, (const float *)m->image->data, 1);
@@ -513,12 +559,22 @@ static int draw_start(SpPhaser *ph, int flags, Image *m) {
 
 static int finish_init_model(SpPhaser *ph, int flags, int rc) {
   if (!rc && (flags & SpModelMaskedOutZeroed)) rc = spb_ctx_mask_out_unmeasured(state(ph)->ctx);
-  if (rc) return dev_error("init model");
-  /* host copy is fetched on the first sp_phaser_model() (model_iteration -1) */
-  ph->model = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  if (rc) {
+    free_spare_model_images(ph);
+    return dev_error("init model");
+  }
+  /* host copy is fetched on the first sp_phaser_model() (model_iteration -1);
+   * the images of the previous start are reused (same dimensions) */
+  dev_state *s = state(ph);
+  ph->model = s->spare_model ? s->spare_model : sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  ph->model_change = s->spare_change ? s->spare_change : sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  s->spare_model = s->spare_change = NULL;
+  if (!s->pinned_model &&
+      !spb_host_register(ph->model->image->data, sizeof(Complex) * (size_t)ph->image_size))
+    s->pinned_model = ph->model->image->data;
   ph->model->phased = 1;
   ph->model_iteration = -1;
-  ph->model_change = sp_image_alloc(ph->nx, ph->ny, ph->nz);
+  ph->model_change_iteration = -1;
   return 0;
 }
 
@@ -528,8 +584,7 @@ static int init_models_check(SpPhaser *ph, int flags) {
     snprintf(g_last_err, sizeof(g_last_err), "sp_phaser_init must succeed before sp_phaser_init_model");
     return -3;
   }
-  if (ph->model) { sp_image_free(ph->model); ph->model = NULL; }
-  if (ph->model_change) { sp_image_free(ph->model_change); ph->model_change = NULL; }
+  release_model_images(ph);
   if (!(flags & (SpModelRandomPhases | SpModelZeroPhases | SpModelRandomValues))) return -3;
   if (!ph->amplitudes) return -3;
   if (sync_to_device(ph)) return -8;
@@ -601,8 +656,8 @@ int sp_phaser_set_starts(SpPhaser *ph, int starts) {
   }
   s->starts = starts;
   s->flags_dev_newer = 0;
-  if (ph->model) { sp_image_free(ph->model); ph->model = NULL; }
-  if (ph->model_change) { sp_image_free(ph->model_change); ph->model_change = NULL; }
+  release_model_images(ph);
+  free_spare_model_images(ph);
   ph->model_iteration = ph->fmodel_iteration = ph->model_before_projection_iteration = -1;
   ph->old_model_iteration = ph->support_iteration = -1;
   return 0;

@@ -232,6 +232,8 @@ struct spb_ctx {
   long long *hard = nullptr;      // random starts: elements the host evaluates (spb_ctx_models_from_phases)
   unsigned *hard_n = nullptr;
   unsigned long long *seeds = nullptr;  // per-start generator keys (device starts)
+  void *hstage = nullptr;               // pinned host staging buffer (spb_ctx_host_stage)
+  size_t hstage_bytes = 0;
   int x_valid = 0, xf_valid = 0;
   float xf_gamma1 = 0.0f;
   int tune[SPB_TUNE_KNOBS] = {};  // launch-shape choices (0: built-in)
@@ -648,6 +650,7 @@ extern "C" void spb_ctx_destroy(spb_ctx *c) {
   for (auto &e : c->spar_ev)
     if (e) cudaEventDestroy(e);
   if (c->spar_pinned) cudaFreeHost(c->spar_pinned);
+  if (c->hstage) cudaFreeHost(c->hstage);
   for (auto &row : c->sup_graph)
     for (auto &g : row)
       if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -704,6 +707,46 @@ extern "C" int spb_ctx_set_stream(spb_ctx *c, void *stream) {
   CK(cudaStreamSynchronize(c->st));
   c->st = stream ? (cudaStream_t)stream : c->own_st;
   return 0;
+}
+
+// Pinned host buffer of at least `bytes`, owned by the context: host data
+// written here crosses to the device by DMA at full speed instead of through
+// the driver's pageable staging.  Valid until the next call with a larger
+// size; the caller's copies from it complete before it is handed out again
+// (every upload through it synchronizes the stream).
+extern "C" void *spb_ctx_host_stage(spb_ctx *c, size_t bytes) {
+  if (bytes <= c->hstage_bytes) return c->hstage;
+  if (c->hstage) {
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return nullptr;
+    cudaFreeHost(c->hstage);
+    c->hstage = nullptr;
+    c->hstage_bytes = 0;
+  }
+  const size_t cap = (bytes + 0xFFFFF) & ~(size_t)0xFFFFF;  // whole MiB
+  if (cudaMallocHost(&c->hstage, cap) != cudaSuccess) {
+    cudaGetLastError();
+    c->hstage = nullptr;
+    fail("cudaMallocHost of a %zu-byte staging buffer", cap);
+    return nullptr;
+  }
+  c->hstage_bytes = cap;
+  return c->hstage;
+}
+
+// Page-locks a host range the library owns and reuses (amplitudes, the model
+// image), so its copies run by DMA; 0 on success.  A range that cannot be
+// locked still works through pageable copies.
+extern "C" int spb_host_register(void *p, size_t bytes) {
+  if (!p || !bytes) return -1;
+  if (cudaHostRegister(p, bytes, cudaHostRegisterPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return 0;
+}
+
+extern "C" void spb_host_unregister(void *p) {
+  if (p && cudaHostUnregister(p) != cudaSuccess) cudaGetLastError();
 }
 
 static int upload(spb_ctx *c, void *dst, const void *src, size_t bytes) {
@@ -837,9 +880,10 @@ extern "C" int spb_ctx_set_phased_amplitudes(spb_ctx *c, const float *pa) {
 }
 
 static int put_flags(spb_ctx *c, int start, const int *flags) {
-  std::vector<uint8_t> h((size_t)c->n);
+  uint8_t *h = (uint8_t *)spb_ctx_host_stage(c, (size_t)c->n);
+  if (!h) return -1;
   for (long long i = 0; i < c->n; i++) h[i] = (uint8_t)(flags[i] & 3);
-  return upload(c, c->flags + (size_t)start * c->n, h.data(), (size_t)c->n);
+  return upload(c, c->flags + (size_t)start * c->n, h, (size_t)c->n);
 }
 
 // every start gets these flags; measured bits feed the shared bitmap

@@ -121,3 +121,71 @@ def test_uniform_draw_matches_rand(env, n, seed, skip):
     want = np.array([np.float32(float(libc.rand()) / RAND_MAX) for _ in range(n)], np.float32)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     assert after == libc.rand()
+
+
+def test_concurrent_bulk_draws_take_whole_blocks(env):
+    """Large draws run their spans on the library's pool of host threads; a
+    draw that finds the pool busy with another thread's draw runs on threads
+    of its own.  Either way each draw is one whole block of the sequence: the
+    outputs of concurrent draws are consecutive blocks of n values, in the
+    order the draws took the generator."""
+    import threading
+
+    L, so, libc, libm = env
+    so.spb_random_uniforms.argtypes = [C.c_void_p, C.c_longlong]
+    n, threads, calls = 300000, 4, 2
+    libc.srand(77)
+    want = np.empty(n * threads * calls, np.float32)
+    so.spb_random_uniforms(want.ctypes.data, want.size)
+    blocks = {want[k * n:(k + 1) * n].tobytes(): k for k in range(threads * calls)}
+    libc.srand(77)
+    outs = [[np.empty(n, np.float32) for _ in range(calls)] for _ in range(threads)]
+
+    def work(t):
+        for c in range(calls):
+            so.spb_random_uniforms(outs[t][c].ctypes.data, n)
+
+    th = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    got = sorted(blocks.get(o.tobytes(), -1) for row in outs for o in row)
+    assert got == list(range(threads * calls))
+
+
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded")
+def test_bulk_draw_in_forked_child(env):
+    """A child forked after the pool's threads exist (they are not copied
+    into it) draws on a fresh pool of its own."""
+    import os
+    import time
+
+    L, so, libc, libm = env
+    so.spb_random_uniforms.argtypes = [C.c_void_p, C.c_longlong]
+    n = 400000
+    warm = np.empty(n, np.float32)
+    so.spb_random_uniforms(warm.ctypes.data, n)  # the pool exists in this process now
+    libc.srand(5)
+    want = np.empty(n, np.float32)
+    so.spb_random_uniforms(want.ctypes.data, n)
+    pid = os.fork()
+    if pid == 0:  # child: no pytest machinery, exit status only
+        try:
+            libc.srand(5)
+            got = np.empty(n, np.float32)
+            so.spb_random_uniforms(got.ctypes.data, n)
+            os._exit(0 if np.array_equal(got.view(np.uint32), want.view(np.uint32)) else 3)
+        except BaseException:
+            os._exit(4)
+    deadline = time.time() + 60
+    while True:
+        done, status = os.waitpid(pid, os.WNOHANG)
+        if done:
+            break
+        if time.time() > deadline:
+            os.kill(pid, 9)
+            os.waitpid(pid, 0)
+            pytest.fail("the forked child's draw did not finish")
+        time.sleep(0.05)
+    assert os.WIFEXITED(status) and os.WEXITSTATUS(status) == 0, status
