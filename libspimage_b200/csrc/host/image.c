@@ -433,8 +433,9 @@ static void draw_span(void *arg, int t, long long i0, long long i1) {
     f = f + 1 == RNG_DEG ? 0 : f + 1;
     r = r + 1 == RNG_DEG ? 0 : r + 1;
     const real u = (real)(((double)(int)(val >> 1)) / (double)RAND_MAX);
-    s->out[i] = s->phases ? (real)(u * 3.14159265358979323846 * 2) : u;
+    spb_stream_f32(&s->out[i], s->phases ? (real)(u * 3.14159265358979323846 * 2) : u);
   }
+  spb_stream_fence(); /* the values are uploaded next */
 }
 
 /* n consecutive p_drand48() values (phases = 0) or phases (phases = 1) into

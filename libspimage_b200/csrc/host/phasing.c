@@ -297,7 +297,7 @@ static void set_amp_span(void *ctx, int t, long long i0, long long i1) {
   set_amp_job *j = (set_amp_job *)ctx;
   long long masked = 0;
   for (long long i = i0; i < i1; i++) {
-    j->ph->amplitudes->data[i] = sp_real(j->img->image->data[i]);
+    spb_stream_f32(&j->ph->amplitudes->data[i], sp_real(j->img->image->data[i])); /* uploaded next */
     if (j->img->mask->data[i]) {
       j->ph->pixel_flags->data[i] |= SpPixelMeasuredAmplitude;
       masked++;
@@ -305,6 +305,7 @@ static void set_amp_span(void *ctx, int t, long long i0, long long i1) {
       j->ph->pixel_flags->data[i] &= ~SpPixelMeasuredAmplitude;
     }
   }
+  spb_stream_fence();
   j->masked[t] = masked;
 }
 

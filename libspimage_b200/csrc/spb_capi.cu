@@ -23,6 +23,7 @@
 #include <mutex>
 #include <vector>
 
+#include "host/host_internal.h"
 #include "spb_internal.h"
 #include "spb_pointwise.cuh"
 #include "spimage/spb_device.h"
@@ -879,10 +880,38 @@ extern "C" int spb_ctx_set_phased_amplitudes(spb_ctx *c, const float *pa) {
   return upload(c, c->pamp, pa, nc);
 }
 
+// host int flags <-> device byte flags, converted on the host threads
+struct FlagsCopy {
+  const int *in32;
+  uint8_t *out8;
+  const uint8_t *in8;
+  int *out32;
+};
+static void flags_to_bytes(void *ctx, int, long long i0, long long i1) {
+  const FlagsCopy *j = (const FlagsCopy *)ctx;
+  const int *in = j->in32;
+  uint8_t *out = j->out8;
+  long long i = i0;
+#if defined(__SSE2__)  // x86: little-endian
+  for (; i < i1 && (i & 3); i++) out[i] = (uint8_t)(in[i] & 3);
+  // four bytes a store, straight to memory (uploaded next; the stage is page-aligned)
+  for (; i + 4 <= i1; i += 4)
+    spb_stream_u32(out + i, (unsigned)(in[i] & 3) | (unsigned)(in[i + 1] & 3) << 8 | (unsigned)(in[i + 2] & 3) << 16 |
+                                (unsigned)(in[i + 3] & 3) << 24);
+#endif
+  for (; i < i1; i++) out[i] = (uint8_t)(in[i] & 3);
+  spb_stream_fence();
+}
+static void bytes_to_flags(void *ctx, int, long long i0, long long i1) {
+  const FlagsCopy *j = (const FlagsCopy *)ctx;
+  for (long long i = i0; i < i1; i++) j->out32[i] = j->in8[i];
+}
+
 static int put_flags(spb_ctx *c, int start, const int *flags) {
   uint8_t *h = (uint8_t *)spb_ctx_host_stage(c, (size_t)c->n);
   if (!h) return -1;
-  for (long long i = 0; i < c->n; i++) h[i] = (uint8_t)(flags[i] & 3);
+  FlagsCopy job = {flags, h, nullptr, nullptr};
+  spb_parallel_for(c->n, flags_to_bytes, &job);
   return upload(c, c->flags + (size_t)start * c->n, h, (size_t)c->n);
 }
 
@@ -911,9 +940,11 @@ extern "C" int spb_ctx_set_start_flags(spb_ctx *c, int start, const int *flags) 
 
 extern "C" int spb_ctx_get_start_flags(spb_ctx *c, int start, int *flags) {
   if (check_start(c, start)) return -1;
-  std::vector<uint8_t> h((size_t)c->n);
-  if (download(c, h.data(), c->flags + (size_t)start * c->n, (size_t)c->n)) return -1;
-  for (long long i = 0; i < c->n; i++) flags[i] = h[i];
+  uint8_t *h = (uint8_t *)spb_ctx_host_stage(c, (size_t)c->n);
+  if (!h) return -1;
+  if (download(c, h, c->flags + (size_t)start * c->n, (size_t)c->n)) return -1;
+  FlagsCopy job = {nullptr, nullptr, h, flags};
+  spb_parallel_for(c->n, bytes_to_flags, &job);
   return 0;
 }
 
