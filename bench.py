@@ -77,7 +77,8 @@ WORKLOADS = {
 
 # launch-shape knobs of spb_ctx_set_tuning by name (--tune; they change no
 # arithmetic): for timing and profiling the other kernel forms
-TUNE_KNOBS = {"row_lines": 0, "no_pdl": 1, "row_g0": 2, "split": 3, "persist": 4, "col_width": 5, "tma": 6, "plane": 7}
+TUNE_KNOBS = {"row_lines": 0, "no_pdl": 1, "row_g0": 2, "split": 3, "persist": 4, "col_width": 5, "tma": 6, "plane": 7,
+              "select": 8}
 
 
 def parse_tune(items):

@@ -105,7 +105,12 @@ const char *spb_kernel_name(int kind);
  * volume with ny = nz = 64 or 128 runs the y and z parts of an iteration --
  * 2 as one plane pass (one block per x-plane: forward y, forward z,
  * projection, inverse z, inverse y; measured slower than the column passes
- * on the B200), 0 (the built-in choice) or 1 as three column passes.
+ * on the B200), 0 (the built-in choice) or 1 as three column passes;
+ * SPB_TUNE_SELECT: how a support update selects and masks -- 2 in one
+ * launch over a cluster of thread blocks per start where the start's |blur|
+ * fits the cluster's shared memory (up to 327,680 pixels; measured no faster
+ * on the B200), 0 (the built-in choice) or 1 with one launch per radix pass
+ * and one for the mask.
  * Setting a knob drops the context's captured graphs. */
 enum {
   SPB_TUNE_ROW_LINES = 0,
@@ -116,7 +121,8 @@ enum {
   SPB_TUNE_COL_WIDTH = 5,
   SPB_TUNE_TMA = 6,
   SPB_TUNE_PLANE = 7,
-  SPB_TUNE_KNOBS = 8
+  SPB_TUNE_SELECT = 8,
+  SPB_TUNE_KNOBS = 9
 };
 int spb_ctx_set_tuning(spb_ctx *ctx, int knob, int value);
 int spb_ctx_get_tuning(spb_ctx *ctx, int knob);

@@ -1470,7 +1470,17 @@ static long long area_rank(long long n, float area) {
 // it at run time (captured support updates).  pdl: launch with programmatic
 // dependent launch (context streams with it enabled).
 static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *absv, long long n, int nb, int type,
-                              float value, uint8_t *flags, const SupportParams *dev = nullptr, bool pdl = false) {
+                              float value, uint8_t *flags, const SupportParams *dev = nullptr, bool pdl = false,
+                              bool cluster = false) {
+  if (cluster && select_cluster_fits(n) && (type == SPB_SUPPORT_AREA || type == SPB_SUPPORT_THRESHOLD)) {
+    const bool area = type == SPB_SUPPORT_AREA;
+    const cudaError_t e = launch_select_mask_cluster(
+        absv, n, nb, area ? 0 : 1, area ? (unsigned long long)area_rank(n, value) : 0ULL,
+        area && dev ? &dev->rank : nullptr, area ? 0.0f : value, !area && dev ? &dev->rel : nullptr, sel, flags, st,
+        pdl);
+    if (e == cudaSuccess) return 0;
+    if (e != cudaErrorNotSupported) CK(e);
+  }
   if (type == SPB_SUPPORT_AREA) {
     CK(launch_select_kth_desc(absv, n, nb, area_rank(n, value), sel, st, dev ? &dev->rank : nullptr, pdl));
     CK(launch_mask_from_abs(absv, sel, 0.0f, 0, flags, n, nb, st, nullptr, pdl));
@@ -1486,8 +1496,11 @@ static int select_and_mask_on(cudaStream_t st, SelectState *sel, const float *ab
 static int select_and_mask(spb_ctx *c, const float *absv, long long n, int nb, int type, float value,
                            uint8_t *flags, const SupportParams *dev = nullptr) {
   if (prof_begin(c)) return -1;
-  if (select_and_mask_on(c->st, c->sel, absv, n, nb, type, value, flags, dev, c->tune[SPB_TUNE_NO_PDL] == 0)) return -1;
-  c->launches += (type == SPB_SUPPORT_AREA) ? 6 : 4;  // init, four histogram passes, mask | init, max, finish, mask
+  const bool cluster = c->tune[SPB_TUNE_SELECT] == 2 && select_cluster_fits(n);
+  if (select_and_mask_on(c->st, c->sel, absv, n, nb, type, value, flags, dev, c->tune[SPB_TUNE_NO_PDL] == 0, cluster))
+    return -1;
+  // one cluster launch | init, four histogram passes, mask | init, max, finish, mask
+  c->launches += cluster ? 1 : (type == SPB_SUPPORT_AREA) ? 6 : 4;
   return prof_end(c, type == SPB_SUPPORT_AREA ? 16 : 17);
 }
 

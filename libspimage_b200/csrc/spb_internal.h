@@ -159,6 +159,15 @@ cudaError_t launch_select_kth_desc(const float *absv, long long n, int nb, long 
 cudaError_t launch_max_abs(const float *absv, long long n, int nb, SelectState *state, cudaStream_t st, bool pdl);
 cudaError_t launch_mask_from_abs(const float *absv, SelectState *state, float rel, int use_rel, uint8_t *flags,
                                  long long n, int nb, cudaStream_t st, const float *rel_dev, bool pdl);
+// The selection and mask of every start in one launch over a thread-block
+// cluster per start (area rule: use_rel 0, k-th largest at rank or *rank_dev;
+// threshold rule: use_rel 1, maximum times rel or *rel_dev), where a start's
+// keys fit the cluster's shared memory (select_cluster_fits); else
+// cudaErrorNotSupported and nothing is launched.
+bool select_cluster_fits(long long n);
+cudaError_t launch_select_mask_cluster(const float *absv, long long n, int nb, int use_rel, unsigned long long rank,
+                                       const unsigned long long *rank_dev, float rel, const float *rel_dev,
+                                       SelectState *state, uint8_t *flags, cudaStream_t st, bool pdl);
 // out[b*4 + k]; scratch of reduce_scratch_doubles(nb) doubles starting at out
 int reduce_scratch_doubles(int nb);
 cudaError_t launch_reduce_efourier(const float2 *F, const float *amp, const uint8_t *flags, long long n, int nb,

@@ -11,6 +11,8 @@
 // when the FFT does.
 #include <math.h>
 
+#include <cooperative_groups.h>
+
 #include "spb_internal.h"
 #include "spb_passes.cuh"
 #include "spb_pointwise.cuh"
@@ -499,11 +501,14 @@ __device__ void select_pick_warp(const unsigned int *hist, unsigned long long ra
     c[j] = hist[lane * 8 + j];
     own += c[j];
   }
-  unsigned long long above = 0;
-  for (int l = 31; l > 0; l--) {
-    const unsigned long long x = __shfl_sync(0xffffffffu, own, l);
-    if (l > lane) above += x;
+  // keys with a larger digit than lane's: the suffix sum over the higher lanes
+  unsigned long long suf = own;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long x = __shfl_down_sync(0xffffffffu, suf, o);
+    if (lane + o < 32) suf += x;
   }
+  const unsigned long long above = suf - own;
   if (lane == 0) {  // unchanged unless a lane finds the digit (it always does: rank < the count)
     out[0] = prefix;
     out[1] = mask;
@@ -691,6 +696,171 @@ cudaError_t launch_mask_from_abs(const float *absv, SelectState *state, float re
                                  long long n, int nb, cudaStream_t st, const float *rel_dev, bool pdl) {
   return launch_maybe_pdl(mask_kernel, dim3(blocks_per_start(n, nb), nb), dim3(256), 0, st, pdl, absv, state, rel,
                           use_rel, flags, n, rel_dev);
+}
+
+// ------------------------------------- one-launch selection over a cluster
+// The support selection and mask of a start whose |blur| fits in the shared
+// memory of one thread-block cluster: the SEL_CLUSTER blocks of the cluster
+// each load a contiguous slice of the start's keys once, then
+//   area rule: four radix passes, each a histogram of the block's slice that
+//   the cluster's blocks read from one another's shared memory (distributed
+//   shared memory) after a cluster barrier; every block sums them in the same
+//   order and picks the same digit (select_pick_warp, as the launch-per-pass
+//   path), so all blocks hold the same k-th largest key after the fourth;
+//   threshold rule: each block's maximum (NaN skipped, as max_abs_kernel),
+//   exchanged the same way, times rel;
+// and each block writes the inside bit of its slice (strict '>', as
+// mask_kernel).  The same key is found as by the launch-per-pass path (the
+// k-th largest key is one value), so the same flags.  One launch replaces
+// six (area) or four (threshold), and the keys are read from memory once
+// instead of five times.  Every block runs the same cluster barriers
+// (no early exit); the last keeps each block's shared memory alive until no
+// block reads it any more.  The grid's y dimension runs over starts.
+#define SEL_CLUSTER 8
+#define SEL_CLUSTER_THREADS 1024
+#define SEL_CLUSTER_MAX_SLICE 40960  // keys per block: 160 KiB of shared memory
+
+namespace cg = cooperative_groups;
+
+static size_t sel_cluster_smem(long long slice) {
+  return sizeof(unsigned int) * ((size_t)slice + 8 * SEL_BINS + 2 * SEL_BINS + SEL_BINS);
+}
+
+__global__ void __launch_bounds__(SEL_CLUSTER_THREADS) select_mask_cluster_kernel(
+    const float *__restrict__ v, long long n, long long slice, SelectState *states, uint8_t *flags, int use_rel,
+    float rel, const float *rel_dev, unsigned long long rank, const unsigned long long *rank_dev) {
+  extern __shared__ unsigned int sel_smem[];
+  unsigned int *keys = sel_smem;                       // [slice]
+  unsigned int *sub = keys + slice;                    // [8][SEL_BINS] partial histograms
+  unsigned int *hout = sub + 8 * SEL_BINS;             // [2][SEL_BINS] the block's histogram, read by the cluster
+  unsigned int *hsum = hout + 2 * SEL_BINS;            // [SEL_BINS] the cluster's histogram
+  __shared__ unsigned int pm[2];
+  __shared__ unsigned long long pr;
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned int crank = cluster.block_rank();
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int b = blockIdx.y;
+  SelectState *s = states + b;
+  const long long i0 = (long long)crank * slice;
+  const long long cnt = i0 >= n ? 0 : (n - i0 < slice ? n - i0 : slice);
+  v += (long long)b * n + i0;
+  flags += (long long)b * n + i0;
+
+  pdl_wait();
+  pdl_release();
+  for (long long i = tid; i < cnt; i += SEL_CLUSTER_THREADS) keys[i] = __float_as_uint(v[i]);
+  const long long rounds = (cnt + SEL_CLUSTER_THREADS - 1) / SEL_CLUSTER_THREADS;
+
+  float t;
+  if (use_rel) {
+    unsigned int m = 0;
+    __syncthreads();
+    for (long long i = tid; i < cnt; i += SEL_CLUSTER_THREADS)
+      if (!isnan(__uint_as_float(keys[i]))) m = max(m, keys[i]);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (tid == 0) hout[0] = 0;
+    __syncthreads();
+    if (lane == 0) atomicMax(&hout[0], m);
+    cluster.sync();  // every block's maximum is in its hout[0]
+    if (tid == 0) {
+      unsigned int mx = 0;
+      for (unsigned int r = 0; r < SEL_CLUSTER; r++) mx = max(mx, *cluster.map_shared_rank(&hout[0], r));
+      pm[0] = mx;
+      if (crank == 0) s->result = __uint_as_float(mx);
+    }
+    __syncthreads();
+    t = __fmul_rn(__uint_as_float(pm[0]), rel_dev ? *rel_dev : rel);
+  } else {
+    if (tid == 0) {
+      pm[0] = 0;  // prefix
+      pm[1] = 0;  // mask
+      pr = rank_dev ? *rank_dev : rank;
+    }
+    for (int pass = 0; pass < 4; pass++) {
+      for (int i = tid; i < 8 * SEL_BINS; i += SEL_CLUSTER_THREADS) sub[i] = 0;
+      __syncthreads();  // keys loaded, partial histograms clear, prefix of this pass set
+      const int shift = 24 - SEL_BITS * pass;
+      const unsigned int prefix = pm[0], pmask = pm[1];
+      unsigned int *h = sub + (warp & 7) * SEL_BINS;
+      for (long long r = 0; r < rounds; r++) {
+        const long long i = r * SEL_CLUSTER_THREADS + tid;
+        const unsigned int key = i < cnt ? keys[i] : 0u;
+        const int digit = (i < cnt && (key & pmask) == prefix) ? (int)((key >> shift) & (SEL_BINS - 1)) : -1;
+        if (__ballot_sync(0xffffffffu, digit >= 0) == 0u) continue;  // warp-uniform
+        const unsigned int peers = __match_any_sync(0xffffffffu, digit);
+        if (digit >= 0 && lane == __ffs(peers) - 1) atomicAdd(&h[digit], (unsigned)__popc(peers));
+      }
+      __syncthreads();
+      unsigned int *ho = hout + (pass & 1) * SEL_BINS;
+      for (int d = tid; d < SEL_BINS; d += SEL_CLUSTER_THREADS) {
+        unsigned int c = 0;
+        for (int w = 0; w < 8; w++) c += sub[w * SEL_BINS + d];
+        ho[d] = c;
+      }
+      // hout[pass & 1] of every block is complete; the buffer of the pass
+      // before was last read before this barrier, so the next pass may reuse it
+      cluster.sync();
+      for (int d = tid; d < SEL_BINS; d += SEL_CLUSTER_THREADS) {
+        unsigned int c[SEL_CLUSTER];
+#pragma unroll
+        for (unsigned int r = 0; r < SEL_CLUSTER; r++) c[r] = *cluster.map_shared_rank(&ho[d], r);  // all in flight
+        unsigned int t = 0;
+#pragma unroll
+        for (unsigned int r = 0; r < SEL_CLUSTER; r++) t += c[r];
+        hsum[d] = t;
+      }
+      __syncthreads();
+      // the narrowed prefix, mask and rank for the next pass (its arguments are
+      // copies, so it may write them in place; the other warps read them after
+      // the barrier)
+      if (warp == 0) select_pick_warp(hsum, pr, prefix, pmask, shift, pm, &pr);
+      __syncthreads();
+    }
+    t = __uint_as_float(pm[0]);
+    if (tid == 0 && crank == 0) s->result = t;
+  }
+  for (long long i = tid; i < cnt; i += SEL_CLUSTER_THREADS) {
+    const uint8_t f = flags[i];
+    flags[i] = (__uint_as_float(keys[i]) > t) ? (uint8_t)(f | FLAG_INSIDE) : (uint8_t)(f & ~FLAG_INSIDE);
+  }
+  cluster.sync();  // no block exits while another may still read its histograms
+}
+
+bool select_cluster_fits(long long n) { return n > 0 && (n + SEL_CLUSTER - 1) / SEL_CLUSTER <= SEL_CLUSTER_MAX_SLICE; }
+
+cudaError_t launch_select_mask_cluster(const float *absv, long long n, int nb, int use_rel, unsigned long long rank,
+                                       const unsigned long long *rank_dev, float rel, const float *rel_dev,
+                                       SelectState *state, uint8_t *flags, cudaStream_t st, bool pdl) {
+  if (!select_cluster_fits(n) || nb < 1 || nb > 65535) return cudaErrorNotSupported;
+  static bool attr_set[64] = {};  // per device
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorNotSupported;
+  const long long slice = (n + SEL_CLUSTER - 1) / SEL_CLUSTER;
+  const size_t smem = sel_cluster_smem(slice);
+  if (!attr_set[dev]) {
+    e = cudaFuncSetAttribute(select_mask_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sel_cluster_smem(SEL_CLUSTER_MAX_SLICE));
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(SEL_CLUSTER, nb);
+  cfg.blockDim = dim3(SEL_CLUSTER_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = SEL_CLUSTER;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 2 : 1;
+  return cudaLaunchKernelEx(&cfg, select_mask_cluster_kernel, absv, n, slice, state, flags, use_rel, rel, rel_dev,
+                            rank, rank_dev);
 }
 
 // ---------------------------------------------------------------- reductions
