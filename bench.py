@@ -708,8 +708,9 @@ def e2e_run(args, L, wl, amp, mask, support, rank, world, torch, dist):
     L.free_image(amp_img)
     L.free_image(sup_img)
     slots = slots_per_step(wl)
-    # per step: amplitudes (4N) + pixel flags (1N) + random-phase start (8N) up; model (8N) down
-    h2d = 4 * n + n + 8 * n
+    # per step up: amplitudes (4N), pixel flags (1N, once: measured and support
+    # bits together), the random-phase start's float phases (4N); down: model (8N)
+    h2d = 4 * n + n + 4 * n
     d2h = 8 * n + 4 * 8
     return world * args.steps * slots / total, h2d, d2h, efour
 

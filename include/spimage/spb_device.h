@@ -142,7 +142,15 @@ int spb_ctx_set_margins(spb_ctx *ctx, const float *amp_min, const float *amp_max
 int spb_ctx_set_phased_amplitudes(spb_ctx *ctx, const float *phased_amp);
 /* pixel flags as the reference's int32 SpPhasingPixelFlags bits */
 int spb_ctx_set_flags(spb_ctx *ctx, const int *flags);
+/* Only the flag bits in `bits` (SpPhasingPixelFlags) from `flags`, every
+ * start, the other bits kept as the device has them (no reference
+ * counterpart: the host API uploads only the bits it edited, so support
+ * bits a support update changed on the device need not come back first). */
+int spb_ctx_set_flags_bits(spb_ctx *ctx, const int *flags, int bits);
 int spb_ctx_get_flags(spb_ctx *ctx, int *flags);
+/* Start 0's flag bits in `bits` into `flags`, the other bits of `flags` kept
+ * (no reference counterpart; the counterpart of spb_ctx_set_flags_bits). */
+int spb_ctx_get_flags_bits(spb_ctx *ctx, int *flags, int bits);
 
 /* Model initialisation (src/phasing.c:606-724; CUDA src/phasing.cu:184-240):
  * set_model copies g1; model_from_fourier sets g1 = IFFT(F)/N; both clear g0

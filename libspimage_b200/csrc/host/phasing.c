@@ -17,11 +17,20 @@
 #include "spimage/spb_device.h"
 #include "host_internal.h"
 
+#define FLAG_BITS ((unsigned)(SpPixelInsideSupport | SpPixelMeasuredAmplitude))
+
 typedef struct {
   spb_ctx *ctx;
   int starts; /* independent reconstructions in the context (0 = 1) */
-  int amp_dirty, flags_dirty, margins_dirty, pamp_dirty;
-  int flags_dev_newer; /* device flags changed by a support update */
+  int amp_dirty, margins_dirty, pamp_dirty;
+  /* Pixel flags live on the host (ph->pixel_flags) and on the device.  The
+   * host edits whole bit classes (every pixel's measured bit, or every
+   * pixel's support bit); support updates change support bits on the
+   * device.  Each side tracks the bits it holds newer values of, so that only
+   * those cross: host_bits go up before the device uses the flags, dev_bits
+   * come down before the host reads them.  The two sets never overlap. */
+  unsigned flags_host_bits;
+  unsigned flags_dev_bits;
   void *pinned_amp;    /* ph->amplitudes->data when page-locked */
   void *pinned_model;  /* ph->model->image->data when page-locked */
   Image *spare_model, *spare_change; /* the previous start's images while a new start is made */
@@ -86,31 +95,47 @@ static int ensure_ctx(SpPhaser *ph) {
   if (spb_ctx_create_batch(&s->ctx, ph->nx, ph->ny, ph->nz, s->starts > 0 ? s->starts : 1))
     return dev_error("device context");
   s->amp_dirty = ph->amplitudes != NULL;
-  s->flags_dirty = ph->pixel_flags != NULL;
+  s->flags_host_bits = ph->pixel_flags != NULL ? FLAG_BITS : 0u; /* a fresh context has none */
+  s->flags_dev_bits = 0;
   s->margins_dirty = ph->amplitudes_min != NULL;
   s->pamp_dirty = ph->phased_amplitudes != NULL;
   return 0;
 }
 
-/* pull support bits changed on the device before the host edits the flags */
+/* pull the flag bits the device changed before the host reads the flags */
 static int sync_flags_to_host(SpPhaser *ph) {
   dev_state *s = state(ph);
-  if (!s->ctx || !s->flags_dev_newer || !ph->pixel_flags) return 0;
-  if (spb_ctx_get_flags(s->ctx, ph->pixel_flags->data)) return dev_error("download pixel flags");
-  s->flags_dev_newer = 0;
+  if (!s->ctx || !s->flags_dev_bits || !ph->pixel_flags) return 0;
+  if (spb_ctx_get_flags_bits(s->ctx, ph->pixel_flags->data, (int)s->flags_dev_bits))
+    return dev_error("download pixel flags");
+  s->flags_dev_bits = 0;
   return 0;
 }
 
-static int sync_to_device(SpPhaser *ph) {
+/* the host has just rewritten `bits` of every pixel's flags */
+static void host_wrote_flags(SpPhaser *ph, unsigned bits) {
+  dev_state *s = state(ph);
+  s->flags_host_bits |= bits;
+  s->flags_dev_bits &= ~bits;
+}
+
+/* the device has changed `bits` of the flags (support updates) */
+static void device_wrote_flags(SpPhaser *ph, unsigned bits) { state(ph)->flags_dev_bits |= bits; }
+
+/* need_flags = 0: the caller's device work reads no pixel flags, so edited
+ * flag bits may wait for a later call (a new start is typically followed by
+ * a new support before the iterations) */
+static int sync_to_device_for(SpPhaser *ph, int need_flags) {
   if (ensure_ctx(ph)) return -8;
   dev_state *s = state(ph);
   if (s->amp_dirty && ph->amplitudes) {
     if (spb_ctx_set_amplitudes(s->ctx, ph->amplitudes->data)) return dev_error("upload amplitudes");
     s->amp_dirty = 0;
   }
-  if (s->flags_dirty && ph->pixel_flags) {
-    if (spb_ctx_set_flags(s->ctx, ph->pixel_flags->data)) return dev_error("upload pixel flags");
-    s->flags_dirty = 0;
+  if (s->flags_host_bits && ph->pixel_flags && need_flags) {
+    if (spb_ctx_set_flags_bits(s->ctx, ph->pixel_flags->data, (int)s->flags_host_bits))
+      return dev_error("upload pixel flags");
+    s->flags_host_bits = 0;
   }
   if (s->margins_dirty && ph->amplitudes_min && ph->amplitudes_max) {
     if (spb_ctx_set_margins(s->ctx, ph->amplitudes_min->data, ph->amplitudes_max->data))
@@ -124,6 +149,8 @@ static int sync_to_device(SpPhaser *ph) {
   }
   return 0;
 }
+
+static int sync_to_device(SpPhaser *ph) { return sync_to_device_for(ph, 1); }
 
 /* ------------------------------------------------------------- algorithms */
 
@@ -264,10 +291,9 @@ void sp_phaser_set_support(SpPhaser *ph, const Image *support) {
   phaser_check_dimensions(ph, support);
   ph->support_iteration = -1;
   ensure_flags(ph);
-  sync_flags_to_host(ph);
-  support_job job = {ph, support};
+  support_job job = {ph, support}; /* every pixel's support bit: no need to fetch the device's first */
   spb_parallel_for(ph->image_size, support_span, &job);
-  state(ph)->flags_dirty = 1;
+  host_wrote_flags(ph, SpPixelInsideSupport);
 }
 
 /* phasing.c:235-269 */
@@ -275,14 +301,13 @@ void sp_phaser_set_phased_amplitudes(SpPhaser *ph, const Image *pa) {
   phaser_check_dimensions(ph, pa);
   if (!ph->phased_amplitudes) ph->phased_amplitudes = sp_c3matrix_alloc(ph->nx, ph->ny, ph->nz);
   ensure_flags(ph);
-  sync_flags_to_host(ph);
   for (int i = 0; i < ph->image_size; i++) {
     ph->phased_amplitudes->data[i] = pa->image->data[i];
     if (pa->mask->data[i]) ph->pixel_flags->data[i] |= SpPixelMeasuredAmplitude;
     else ph->pixel_flags->data[i] &= ~SpPixelMeasuredAmplitude;
   }
   state(ph)->pamp_dirty = 1;
-  state(ph)->flags_dirty = 1;
+  host_wrote_flags(ph, SpPixelMeasuredAmplitude);
 }
 
 /* phasing.c:294-333 */
@@ -317,14 +342,13 @@ void sp_phaser_set_amplitudes(SpPhaser *ph, const Image *amplitudes) {
       state(ph)->pinned_amp = ph->amplitudes->data;
   }
   ensure_flags(ph);
-  sync_flags_to_host(ph);
-  set_amp_job job = {ph, amplitudes, {0}};
+  set_amp_job job = {ph, amplitudes, {0}}; /* every pixel's measured bit */
   const int spans = spb_parallel_for(ph->image_size, set_amp_span, &job);
   long long masked = 0;
   for (int t = 0; t < spans; t++) masked += job.masked[t];
   if (masked == 0) fprintf(stderr, "Amplitudes mask is all zeros!\n");
   state(ph)->amp_dirty = 1;
-  state(ph)->flags_dirty = 1;
+  host_wrote_flags(ph, SpPixelMeasuredAmplitude);
 }
 
 /* phasing.c:335-363 */
@@ -493,7 +517,8 @@ int sp_phaser_init_model(SpPhaser *ph, const Image *user_model, int flags) {
   release_model_images(ph);
   if (!user_model && !(flags & (SpModelRandomPhases | SpModelZeroPhases | SpModelRandomValues))) return -3;
   if (user_model) phaser_check_dimensions(ph, user_model);
-  if (sync_to_device(ph)) return -8;
+  /* only a masked-out start reads the pixel flags */
+  if (sync_to_device_for(ph, (flags & SpModelMaskedOutZeroed) != 0)) return -8;
   spb_ctx *ctx = state(ph)->ctx;
   int rc = 0;
   if (user_model) {
@@ -588,7 +613,7 @@ static int init_models_check(SpPhaser *ph, int flags) {
   release_model_images(ph);
   if (!(flags & (SpModelRandomPhases | SpModelZeroPhases | SpModelRandomValues))) return -3;
   if (!ph->amplitudes) return -3;
-  if (sync_to_device(ph)) return -8;
+  if (sync_to_device_for(ph, (flags & SpModelMaskedOutZeroed) != 0)) return -8;
   return 0;
 }
 
@@ -656,7 +681,7 @@ int sp_phaser_set_starts(SpPhaser *ph, int starts) {
     s->ctx = NULL;
   }
   s->starts = starts;
-  s->flags_dev_newer = 0;
+  s->flags_dev_bits = 0;
   release_model_images(ph);
   free_spare_model_images(ph);
   ph->model_iteration = ph->fmodel_iteration = ph->model_before_projection_iteration = -1;
@@ -744,10 +769,9 @@ int sp_phaser_init_support(SpPhaser *ph, const Image *support, int flags, real v
   if (support) {
     phaser_check_dimensions(ph, support);
     ensure_flags(ph);
-    sync_flags_to_host(ph);
-    support_job job = {ph, support};
+    support_job job = {ph, support}; /* every pixel's support bit */
     spb_parallel_for(ph->image_size, support_span, &job);
-    state(ph)->flags_dirty = 1;
+    host_wrote_flags(ph, SpPixelInsideSupport);
     ph->support_iteration = -1;
     return 0;
   }
@@ -755,7 +779,7 @@ int sp_phaser_init_support(SpPhaser *ph, const Image *support, int flags, real v
     ensure_flags(ph);
     if (sync_to_device(ph)) return -8;
     if (spb_ctx_support_patterson(state(ph)->ctx, value)) return dev_error("Patterson support");
-    state(ph)->flags_dev_newer = 1;
+    device_wrote_flags(ph, SpPixelInsideSupport);
     ph->support_iteration = -1;
     return 0;
   }
@@ -859,7 +883,7 @@ int sp_phaser_iterate(SpPhaser *ph, int iterations) {
 
 /* phasing.c:803-832 (sums in double on the device) */
 real sp_phaser_ereal(SpPhaser *ph) {
-  if (ensure_ctx(ph)) return -8;
+  if (sync_to_device(ph)) return -8; /* the support bits the host last set */
   double s[2];
   if (spb_ctx_ereal_sums(state(ph)->ctx, s)) return dev_error("ereal");
   return (real)sqrt(s[0] / s[1]);
@@ -898,21 +922,21 @@ void *sp_phaser_device_context(SpPhaser *ph) {
 int spb_phaser_support_update(SpPhaser *ph, int type, real radius, real value) {
   if (sync_to_device(ph)) return -8;
   if (spb_ctx_support_update(state(ph)->ctx, type, radius, value)) return dev_error("support update");
-  state(ph)->flags_dev_newer = 1;
+  device_wrote_flags(ph, SpPixelInsideSupport);
   return 0;
 }
 
 int spb_phaser_support_close(SpPhaser *ph, int size) {
   if (sync_to_device(ph)) return -8;
   if (spb_ctx_support_close(state(ph)->ctx, size)) return dev_error("support close");
-  state(ph)->flags_dev_newer = 1;
+  device_wrote_flags(ph, SpPixelInsideSupport);
   return 0;
 }
 
 int spb_phaser_support_from_abs(SpPhaser *ph, const float *abs_values, real threshold) {
   if (sync_to_device(ph)) return -8;
   if (spb_ctx_support_from_abs(state(ph)->ctx, abs_values, threshold)) return dev_error("template support");
-  state(ph)->flags_dev_newer = 1;
+  device_wrote_flags(ph, SpPixelInsideSupport);
   return 0;
 }
 
@@ -1010,6 +1034,6 @@ int spb_phaser_support_centre(SpPhaser *ph) {
   }
   free(f);
   free(tmp);
-  state(ph)->flags_dev_newer = 1;
+  device_wrote_flags(ph, SpPixelInsideSupport);
   return rc;
 }

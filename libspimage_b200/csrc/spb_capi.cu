@@ -804,6 +804,12 @@ __global__ void build_meas_bits_kernel(const uint8_t *flags, uint32_t *bits, int
     bits[k] = word;
   }
 }
+// every start's flag bits in `mask` from the n bytes at src, the other bits kept
+__global__ void merge_flags_kernel(uint8_t *flags, const uint8_t *__restrict__ src, long long n, int nb, uint8_t mask) {
+  const long long total = n * nb;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x)
+    flags[k] = (uint8_t)((flags[k] & ~mask) | (src[k % n] & mask));
+}
 // every start's flags = start 0's (bits in `mask`), keeping the other bits
 __global__ void broadcast_flags_kernel(uint8_t *flags, long long n, int nb, uint8_t mask) {
   const long long total = n * (nb - 1);
@@ -886,6 +892,7 @@ struct FlagsCopy {
   uint8_t *out8;
   const uint8_t *in8;
   int *out32;
+  int bits;  // bytes_to_flags: 0 = whole value, else only these bits (the others kept)
 };
 static void flags_to_bytes(void *ctx, int, long long i0, long long i1) {
   const FlagsCopy *j = (const FlagsCopy *)ctx;
@@ -904,13 +911,18 @@ static void flags_to_bytes(void *ctx, int, long long i0, long long i1) {
 }
 static void bytes_to_flags(void *ctx, int, long long i0, long long i1) {
   const FlagsCopy *j = (const FlagsCopy *)ctx;
-  for (long long i = i0; i < i1; i++) j->out32[i] = j->in8[i];
+  if (!j->bits) {
+    for (long long i = i0; i < i1; i++) j->out32[i] = j->in8[i];
+  } else {
+    const int keep = ~j->bits;
+    for (long long i = i0; i < i1; i++) j->out32[i] = (j->out32[i] & keep) | (j->in8[i] & j->bits);
+  }
 }
 
 static int put_flags(spb_ctx *c, int start, const int *flags) {
   uint8_t *h = (uint8_t *)spb_ctx_host_stage(c, (size_t)c->n);
   if (!h) return -1;
-  FlagsCopy job = {flags, h, nullptr, nullptr};
+  FlagsCopy job = {flags, h, nullptr, nullptr, 0};
   spb_parallel_for(c->n, flags_to_bytes, &job);
   return upload(c, c->flags + (size_t)start * c->n, h, (size_t)c->n);
 }
@@ -928,6 +940,27 @@ extern "C" int spb_ctx_set_flags(spb_ctx *c, const int *flags) {
   return 0;
 }
 
+// Only the flag bits in `bits` from the host (every start), the others kept
+// as the device has them: the host edited those bits alone, and the device
+// may hold newer values of the others (support updates).
+extern "C" int spb_ctx_set_flags_bits(spb_ctx *c, const int *flags, int bits) {
+  bits &= FLAG_INSIDE | FLAG_MEASURED;
+  if (bits == (FLAG_INSIDE | FLAG_MEASURED)) return spb_ctx_set_flags(c, flags);
+  if (!bits) return 0;
+  uint8_t *scratch = (uint8_t *)c->absb;  // n bytes of the support-update scratch, free between calls
+  uint8_t *h = (uint8_t *)spb_ctx_host_stage(c, (size_t)c->n);
+  if (!h) return -1;
+  FlagsCopy job = {flags, h, nullptr, nullptr, 0};
+  spb_parallel_for(c->n, flags_to_bytes, &job);
+  if (upload(c, scratch, h, (size_t)c->n)) return -1;
+  merge_flags_kernel<<<592, 256, 0, c->st>>>(c->flags, scratch, c->n, c->nb, (uint8_t)bits);
+  CK(cudaGetLastError());
+  if ((bits & FLAG_MEASURED) && build_meas_bits(c)) return -1;
+  CK(cudaStreamSynchronize(c->st));
+  c->xf_valid = 0;
+  return 0;
+}
+
 // one start's flags; its measured bits must equal start 0's (one pattern)
 extern "C" int spb_ctx_set_start_flags(spb_ctx *c, int start, const int *flags) {
   if (check_start(c, start)) return -1;
@@ -938,17 +971,24 @@ extern "C" int spb_ctx_set_start_flags(spb_ctx *c, int start, const int *flags) 
   return 0;
 }
 
-extern "C" int spb_ctx_get_start_flags(spb_ctx *c, int start, int *flags) {
+static int get_flags(spb_ctx *c, int start, int *flags, int bits) {
   if (check_start(c, start)) return -1;
   uint8_t *h = (uint8_t *)spb_ctx_host_stage(c, (size_t)c->n);
   if (!h) return -1;
   if (download(c, h, c->flags + (size_t)start * c->n, (size_t)c->n)) return -1;
-  FlagsCopy job = {nullptr, nullptr, h, flags};
+  FlagsCopy job = {nullptr, nullptr, h, flags, bits};
   spb_parallel_for(c->n, bytes_to_flags, &job);
   return 0;
 }
 
-extern "C" int spb_ctx_get_flags(spb_ctx *c, int *flags) { return spb_ctx_get_start_flags(c, 0, flags); }
+extern "C" int spb_ctx_get_start_flags(spb_ctx *c, int start, int *flags) { return get_flags(c, start, flags, 0); }
+
+extern "C" int spb_ctx_get_flags(spb_ctx *c, int *flags) { return get_flags(c, 0, flags, 0); }
+
+extern "C" int spb_ctx_get_flags_bits(spb_ctx *c, int *flags, int bits) {
+  bits &= FLAG_INSIDE | FLAG_MEASURED;
+  return bits ? get_flags(c, 0, flags, bits) : 0;
+}
 
 static int reset_iterates(spb_ctx *c) {
   const size_t nc = sizeof(float2) * (size_t)c->ntot;
