@@ -72,3 +72,20 @@ def test_phaser_support_updates_bit_exact(lib, oracle_mod, shape, alg, sup, star
         ref = setup_pattern(oracle_mod.Restatement(shape, threads=8), pat, alg, 0.87, [sup], seed=40 + (k or 0))
         assert ref.iterate(21) == 0
         assert_same_state(gpu, ref, start=k)
+
+
+@pytest.mark.parametrize("sup", [(AREA, 6, 2.0, 0.1), (THRESHOLD, 6, 1.5, 0.2)], ids=["area", "threshold"])
+def test_large_batch_streaming_select_bit_exact(lib, oracle_mod, sup):
+    """300 starts of 128x128: two blocks per start, so each thread of the
+    histogram and mask launches streams many keys and takes them four at a
+    time (16-byte loads); starts 0 and 299 against the oracle."""
+    shape, starts = (128, 128), 300
+    pat = synth.make_pattern(shape, 32, 1e7, 4.0, seed=23)
+    seeds = list(range(60, 60 + starts))
+    gpu = setup_pattern(lib.Phaser(shape), pat, HIO, 0.9, [sup], seed=60, starts=seeds)
+    gpu.set_tuning(PERSIST, 1)
+    assert gpu.iterate(13) == 0
+    for k in (0, starts - 1):
+        ref = setup_pattern(oracle_mod.Restatement(shape, threads=8), pat, HIO, 0.9, [sup], seed=60 + k)
+        assert ref.iterate(13) == 0
+        assert_same_state(gpu, ref, start=k)
