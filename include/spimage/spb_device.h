@@ -98,7 +98,8 @@ const char *spb_kernel_name(int kind);
  * how the projection pass of 16-point lines of 64 points or more moves its
  * column tiles -- 0 (the built-in choice) with the tensor memory accelerator
  * (bulk tensor loads under an mbarrier and bulk tensor stores) where the
- * tile fits and no other column width is asked for, 2 with it wherever the
+ * tile fits and no other column width is asked for (the blur column pass of
+ * the support updates likewise), 2 with it wherever the
  * tile fits and, in addition, the HIO/RAAR/ER row pass with 1-D bulk copies
  * of its rows (rows of 64 points or more; measured no faster than its plain
  * coalesced loads), 1 with plain loads and stores; SPB_TUNE_PLANE: how a 3-D

@@ -568,6 +568,7 @@ __global__ void __launch_bounds__(256) col_tma_kernel(PassArgs a, const float2 *
   __shared__ __align__(8) uint64_t bar;
   float2 *sm = reinterpret_cast<float2 *>(
       tma_smem_raw + ((kTmaSmemAlign - (smem_u32(tma_smem_raw) & (kTmaSmemAlign - 1))) & (kTmaSmemAlign - 1)));
+  constexpr bool PROJ = MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC;  // else the blur pass
   const int c = threadIdx.x % C, t = threadIdx.x / C;
   const int col0 = blockIdx.x * C;
   // self-check before any copy is issued (uniform over the block): a tile
@@ -590,7 +591,7 @@ __global__ void __launch_bounds__(256) col_tma_kernel(PassArgs a, const float2 *
     mbar_init_fence();
   }
   stage_twiddles<N>(tw_s, stw);
-  {
+  if constexpr (PROJ) {
     const float *asrc = a.amp_line + (size_t)col0 * N;
     for (int k = threadIdx.x; k < C * (N / 4); k += blockDim.x) {
       const int l = k / (N / 4), j = k % (N / 4);
@@ -622,7 +623,8 @@ __global__ void __launch_bounds__(256) col_tma_kernel(PassArgs a, const float2 *
   cp_async_wait_all();
   __syncthreads();  // every tile read (and the operand lines in) before the exchanges reuse the space
   reg::fft<N, false>(v, line, t, tw_s);
-  project16<T, MODE == COL_PROJECT>(v, amp_s + c * SA, meas_s + c * SW, t, lbase, qstride, a);
+  if constexpr (PROJ) project16<T, MODE == COL_PROJECT>(v, amp_s + c * SA, meas_s + c * SW, t, lbase, qstride, a);
+  else blur16<T>(v, col0 + c, o, t, a);
   reg::fft<N, true>(v, line, t, tw_s);
   __syncthreads();  // the exchange lines are free again
 #pragma unroll
@@ -671,17 +673,23 @@ static bool make_tile_map(CUtensorMap *m, const void *base, long long inner, lon
 // columns (C >= 2 columns of 8 bytes, an even column stride), whole tiles
 // (ncols a multiple of C), lines of the tile's length, 16-byte-aligned bases.
 template <int N, int C>
-static bool tma_fits(const PassArgs &a) {
+static bool tma_tile_fits(const PassArgs &a) {
   if (C < 2 || a.ncols % C != 0 || (a.estride & 1) || a.ostride != (long long)N * a.estride) return false;
-  if (((uintptr_t)a.src & 15) || ((uintptr_t)a.dst & 15)) return false;
-  return a.amp_line && a.meas_bits && a.meas_words == proj_words(N);
+  return !((uintptr_t)a.src & 15) && !((uintptr_t)a.dst & 15);
+}
+template <int N, int C>
+static bool tma_fits(const PassArgs &a) {
+  return tma_tile_fits<N, C>(a) && a.amp_line && a.meas_bits && a.meas_words == proj_words(N);
 }
 
 template <int N, int MODE, int C>
 static cudaError_t col_tma_launch(const LinePlan &pl, const PassArgs &a, cudaStream_t st) {
   constexpr int T = N / 16;
+  constexpr bool PROJ = MODE == COL_PROJECT || MODE == COL_PROJECT_NOFC;
   const size_t smem = (size_t)(N + C * (N + N / 16 + (C > 1 ? 16 / C : 0))) * sizeof(float2) +
-                      (size_t)C * amp_stride<N, C>() * sizeof(float) + (size_t)C * bits_stride<N, C>() * sizeof(uint32_t) +
+                      (PROJ ? (size_t)C * amp_stride<N, C>() * sizeof(float) +
+                                  (size_t)C * bits_stride<N, C>() * sizeof(uint32_t)
+                            : 0) +
                       kTmaSmemAlign;  // room to round the block's base up to the copies' alignment
   CUtensorMap tin, tout;
   const long long rows = (a.outer0 + a.nouter) * (long long)N;
@@ -1281,6 +1289,15 @@ static cudaError_t col_fast_launch(const LinePlan &pl, const PassArgs &a, cudaSt
       }
     }
     return col_fast_launch_p<N, MODE, PROJ>(pl, a, st);
+  }
+  if constexpr (MODE == COL_BLUR && N >= 64) {
+    // the blur pass's column tiles by the tensor memory accelerator too
+    // (knob 1: plain loads), at the built-in width
+    constexpr int C = col_width<N>();
+    if (a.tma != 1 && tma_tile_fits<N, C>(a)) {
+      const cudaError_t te = col_tma_launch<N, MODE, C>(pl, a, st);
+      if (te != cudaErrorNotSupported) return te;
+    }
   }
   return col_fast_launch_p<N, MODE, false>(pl, a, st);
 }
