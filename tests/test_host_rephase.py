@@ -189,3 +189,42 @@ def test_bulk_draw_in_forked_child(env):
             pytest.fail("the forked child's draw did not finish")
         time.sleep(0.05)
     assert os.WIFEXITED(status) and os.WEXITSTATUS(status) == 0, status
+
+
+def test_parallel_for_spans_partition_the_range(env):
+    """spb_parallel_for (the host loops of set_amplitudes, init_support and the
+    flag conversions) runs fn over contiguous spans that cover [0, n) exactly
+    once, on the pool or, when another caller holds the pool, on threads of
+    its own; two callers at once both get whole partitions."""
+    import threading
+
+    L, so, libc, libm = env
+    SPAN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_longlong, C.c_longlong)
+    so.spb_parallel_for.argtypes = [C.c_longlong, SPAN, C.c_void_p]
+    so.spb_parallel_for.restype = C.c_int
+    results = {}
+
+    def run(key, n):
+        got = []
+        lock = threading.Lock()
+
+        def fn(ctx, t, i0, i1):
+            with lock:
+                got.append((t, i0, i1))
+
+        cb = SPAN(fn)
+        spans = so.spb_parallel_for(n, cb, None)
+        results[key] = (spans, sorted(got, key=lambda s: s[1]), n)
+
+    for n in (5, 1 << 18, 1000003):
+        run(n, n)
+    th = [threading.Thread(target=run, args=(f"c{k}", 600000 + k)) for k in range(3)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for key, (spans, got, n) in results.items():
+        assert 1 <= spans <= 8 and len(got) == spans, key
+        assert sorted(t for t, _, _ in got) == list(range(spans)), key
+        assert got[0][1] == 0 and got[-1][2] == n, key
+        assert all(a[2] == b[1] for a, b in zip(got, got[1:])), key
